@@ -1,0 +1,192 @@
+"""Host-side binding of the cavity solver's C ABI (ctypes).
+
+This module mirrors the reference's Python binding, `python_api.py:1-161`, name for name: the same
+`Config` / `Report` / `Diagnostics` records (byte layout fixed by backend.cu:584-597 and
+python_api.py:11-28), the same `Solver` methods with the same argument meaning, NumPy shapes and error
+behaviour (a non-zero return code raises `RuntimeError` carrying `solver_last_error()`,
+python_api.py:82-84).  Code written against the reference's binding runs unchanged against this one.
+
+By default it loads `libcavity_solver.so` from this package (the B200 build).  The `library=` argument
+selects another build of the same ABI, e.g. the CPU oracle under `oracle/` or the reference's own
+`backend.cu` built under `oracle/_ref/`; tests use that to drive all three through one code path.
+"""
+import ctypes as ct
+import os
+from pathlib import Path
+
+import numpy as np
+
+PACKAGE_DIR = Path(__file__).resolve().parent
+DEFAULT_LIBRARY = PACKAGE_DIR / 'libcavity_solver.so'
+
+
+class Config(ct.Structure):
+    """Solver settings: 11 int32, 14 double, probe_x[8], probe_y[8]; 288 bytes (backend.cu:584-589)."""
+    _fields_ = ([(name, ct.c_int) for name in
+                 ('nx', 'ny', 'nz', 'lid_shaped', 'impulse_order', 'adaptive_dt', 'dt_lag', 'phi_extrapolate',
+                  'fdm_max_passes', 'grid_stretch', 'n_probes')]
+                + [(name, ct.c_double) for name in
+                   ('length', 'u_lid', 'nu', 'lz', 'lid_ramp_t', 'reinit_r', 'impulse_order4_ramp',
+                    'grid_dx_wall', 'grid_max_aspect', 'dt_fixed', 'dt_max', 'cfl_target', 'diffusion_limit',
+                    'fdm_rtol')]
+                + [('probe_x', ct.c_double * 8), ('probe_y', ct.c_double * 8)])
+
+
+class Report(ct.Structure):
+    """State of the clock after a step: 48 bytes (backend.cu:590-594)."""
+    _fields_ = [('steps', ct.c_longlong), ('time', ct.c_double), ('dt', ct.c_double), ('cfl', ct.c_double),
+                ('phi_rel', ct.c_double), ('dt_reason', ct.c_int), ('phi_passes', ct.c_int)]
+
+
+class Diagnostics(ct.Structure):
+    """Volume-averaged diagnostics: 8 doubles (backend.cu:595-597)."""
+    _fields_ = [(name, ct.c_double) for name in
+                ('kinetic_energy', 'enstrophy', 'umax', 'div_rms', 'cfl_rate', 'gauge_ratio', 'gauge_x', 'gauge_y')]
+
+
+DT_REASONS = ('fixed_DT', 'DT_MAX', 'CFL', 'viscous')
+FIELD_NUMBER = {'u': 0, 'v': 1, 'w': 2, 'mx': 3, 'my': 4, 'mz': 5, 'phi': 6}
+FIELD_NAMES = ('u', 'v', 'w', 'mx', 'my', 'mz', 'phi')
+# precision forms of the B200 build (cavity_set_precision); other builds ignore it
+PRECISION = {'fp64': 0, 'mixed': 1}
+
+
+def pointer(a):
+    """C pointer to a NumPy array's data; None stays None (= NULL)."""
+    return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+def load_library(library=None):
+    """Open a build of the solver ABI and declare the argument types that need one."""
+    library = Path(DEFAULT_LIBRARY if library is None else library)
+    if not library.is_file():
+        raise FileNotFoundError(f'solver library not built: {library} (run __graft_entry__.build())')
+    lib = ct.CDLL(str(library))
+    lib.solver_last_error.restype = ct.c_char_p
+    lib.solver_set_clock.argtypes = [ct.c_double, ct.c_longlong, ct.c_double]
+    lib.solver_kick.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_double, ct.c_int]
+    lib.solver_add_statistics.argtypes = [ct.c_double, ct.c_void_p]
+    if hasattr(lib, 'cavity_set_precision'):
+        lib.cavity_set_precision.argtypes = [ct.c_int]
+    return lib
+
+
+def make_config(settings):
+    """Config record from a settings dict, copying fields by name; `probes` is a list of (x/L, y/L)."""
+    config = Config()
+    for name, _ in Config._fields_:
+        if name in settings:
+            setattr(config, name, settings[name])
+    probes = list(settings.get('probes', ()))[:8]
+    config.n_probes = len(probes)
+    for k, (px, py) in enumerate(probes):
+        config.probe_x[k], config.probe_y[k] = px, py
+    return config
+
+
+class Solver:
+    """One cavity on the device.  Create, `initialize()`, then `step()` in a loop (python_api.py:40-161).
+
+    `precision` selects the form of the B200 build ('fp64' default, or 'mixed'); it is ignored by
+    builds of the ABI that have a single form (the oracle, the reference).
+    """
+
+    def __init__(self, settings, library=None, precision=None):
+        self.lib = load_library(library)
+        if precision is not None and hasattr(self.lib, 'cavity_set_precision'):
+            self.call('cavity_set_precision', PRECISION[precision])
+        config = make_config(settings)
+        self.config = config
+        self.call('solver_create', ct.byref(config))
+        nx, ny, nz = config.nx, config.ny, config.nz
+        self.nx, self.ny, self.nz = nx, ny, nz
+        # NumPy shapes [z, y, x] of every field (python_api.py:73-74)
+        self.shapes = {'u': (nz, ny, nx + 1), 'v': (nz, ny + 1, nx), 'w': (nz + 1, ny, nx), 'phi': (nz, ny, nx)}
+        self.shapes.update(mx=self.shapes['u'], my=self.shapes['v'], mz=self.shapes['w'])
+        self.grid = {}
+        for axis, (name, n) in enumerate((('x', nx), ('y', ny), ('z', nz))):
+            faces, centres = np.empty(n + 1), np.empty(n)
+            self.call('solver_grid', axis, pointer(faces), pointer(centres))
+            self.grid[name] = (faces, centres)
+
+    def call(self, name, *args):
+        if getattr(self.lib, name)(*args):
+            raise RuntimeError(self.lib.solver_last_error().decode())
+
+    def initialize(self, v_noise=None, w_noise=None):
+        v = None if v_noise is None else np.ascontiguousarray(v_noise, dtype=np.float64)
+        w = None if w_noise is None else np.ascontiguousarray(w_noise, dtype=np.float64)
+        self.call('solver_initialize', pointer(v), pointer(w))
+
+    def step(self):
+        r = Report()
+        self.call('solver_step', ct.byref(r))
+        return self._as_dict(r)
+
+    def report(self):
+        r = Report()
+        self.call('solver_report', ct.byref(r))
+        return self._as_dict(r)
+
+    @staticmethod
+    def _as_dict(r):
+        d = {name: getattr(r, name) for name, _ in Report._fields_}
+        d['dt_reason'] = DT_REASONS[r.dt_reason]
+        return d
+
+    def kick(self, noise, amplitude, passes):
+        n = [np.ascontiguousarray(a, dtype=np.float64) for a in noise]
+        self.call('solver_kick', pointer(n[0]), pointer(n[1]), pointer(n[2]), float(amplitude), int(passes))
+
+    def diagnostics(self):
+        d = Diagnostics()
+        self.call('solver_diagnostics', ct.byref(d))
+        return {name: getattr(d, name) for name, _ in Diagnostics._fields_}
+
+    def field(self, name):
+        out = np.empty(self.shapes[name], dtype=np.float64 if name == 'phi' else np.float32)
+        self.call('solver_get_field', FIELD_NUMBER[name], pointer(out))
+        return out
+
+    def set_field(self, name, values):
+        a = np.ascontiguousarray(values, dtype=np.float64 if name == 'phi' else np.float32)
+        if a.shape != self.shapes[name]:
+            raise ValueError(f'{name}: shape {a.shape}, expected {self.shapes[name]}')
+        self.call('solver_set_field', FIELD_NUMBER[name], pointer(a))
+
+    def set_clock(self, time, steps, last_dt):
+        self.call('solver_set_clock', float(time), int(steps), float(last_dt))
+
+    def probes(self):
+        out = np.zeros(2 * self.config.n_probes, dtype=np.float32)
+        self.call('solver_probes', pointer(out))
+        return out
+
+    def add_statistics(self, weight):
+        """Add the mid-span field to the statistics; returns the centreline sample (u, v, uu, vv, ww)."""
+        line = np.empty((5, self.nx))
+        self.call('solver_add_statistics', float(weight), pointer(line))
+        return line
+
+    def statistics(self):
+        sums = np.empty((6, self.ny, self.nx))
+        self.call('solver_get_statistics', pointer(sums))
+        return dict(zip(('u', 'v', 'uu', 'vv', 'ww', 'uv'), sums))
+
+    def set_statistics(self, sums):
+        a = np.ascontiguousarray([sums[k] for k in ('u', 'v', 'uu', 'vv', 'ww', 'uv')], dtype=np.float64)
+        self.call('solver_set_statistics', pointer(a))
+
+    def midplane(self):
+        out = np.empty((4, self.ny, self.nx), dtype=np.float32)
+        self.call('solver_midplane', pointer(out))
+        return out
+
+    def q_volume(self, colour_w=True):
+        q = np.empty((self.nz, self.ny, self.nx), dtype=np.float32)
+        colour = np.empty_like(q)
+        self.call('solver_q_volume', int(bool(colour_w)), pointer(q), pointer(colour))
+        return q, colour
+
+    def close(self):
+        self.call('solver_destroy')
