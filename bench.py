@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Benchmark of the cavity time step on B200: cell-updates/s per SSP-RK3 step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2_64cube_re1000]
+
+A step is one full time step of the solver (3 RK stages, each with its pressure projection) of the seeded
+synthetic workload; the default workload is the plain FP64 form on the 64^3 tanh-stretched cavity (Re 1000,
+regularised lid, adaptive dt at CFL 0.5, noise 1e-3).  `value` is device time (CUDA events on the solver's
+stream around each step, the L2 cache flushed by a 256 MiB write before each timed step), max over ranks;
+`e2e` is the same metric through the reference-facing C ABI (`solver_*`) from host buffers, wall clock,
+host<->device copies included.  With N > 1 (torchrun) every rank advances its own replica cavity (the step has
+no collective); `value` counts all ranks' cells.
+
+--impl reference times the reference's algorithm on the host cores: the OpenMP FP64 restatement under oracle/
+(the reference ships no CPU path), on the same workload, and adds the reference's own backend.cu (built from
+its source under oracle/_ref) on the GPU where that build is present.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=30)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
+    ap.add_argument('--workload', default='c2_64cube_re1000')
+    ap.add_argument('--precision', choices=('fp64', 'mixed'), default=None)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------ ranks
+class Ranks:
+    """torch.distributed plumbing for N replicas (barrier and max over ranks); identity at N = 1."""
+
+    def __init__(self, gpus):
+        self.world = int(os.environ.get('WORLD_SIZE', '1'))
+        self.rank = int(os.environ.get('RANK', '0'))
+        self.local = int(os.environ.get('LOCAL_RANK', '0'))
+        self.pg = None
+        if self.world > 1:
+            # one GPU per rank: make it device 0 of this process before CUDA starts
+            os.environ['CUDA_VISIBLE_DEVICES'] = str(self.local)
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(0)
+            dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120), device_id=torch.device('cuda', 0))
+            self.dist, self.torch = dist, torch
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], device='cuda')
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.QUERY}',
+                                          '--format=csv,noheader,nounits', '-lms', '100'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, max_mhz, reasons = [], None, set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for line in self.lines:
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                max_mhz = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(mhz) if mhz else None, 'sm_max_mhz': max_mhz,
+                'reasons': sorted(reasons), 'samples': len(mhz)}
+
+
+# ------------------------------------------------------------------------------------------ helpers
+def measured_peaks():
+    p = ROOT / 'MEASURED_PEAKS.json'
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def profile_traffic(workload):
+    """DRAM bytes per momentum-sweep launch from the committed ncu summary (None if absent)."""
+    p = ROOT / 'profiles' / f'momentum_sweep_{workload}.md'
+    if not p.is_file():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith('traffic_bytes_per_launch:'):
+            return float(line.split(':', 1)[1])
+    return None
+
+
+def momentum_bytes(settings, field_bytes):
+    """Algorithmic HBM bytes of one momentum-sweep launch: per component 4 face arrays (read u, m and the RK
+    base or write it, write the new impulse), each element once."""
+    nx, ny, nz = settings['nx'], settings['ny'], settings['nz']
+    faces = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+    return 4 * faces * field_bytes
+
+
+def cpu_oracle_rate(workload, steps_budget_s=12.0, max_steps=40):
+    """The FP64 OpenMP oracle on this host: cell-updates/s over a bounded number of steps."""
+    from les_impulse3d_64_b200 import workloads
+    from les_impulse3d_64_b200.api import Solver
+    sys.path.insert(0, str(ROOT / 'oracle'))
+    import build_oracle
+    build_oracle.build_oracle()
+    w = workloads.WORKLOADS[workload]
+    sim = Solver(w['settings'], library=ROOT / 'oracle' / 'libcavity_oracle.so')
+    try:
+        sim.initialize(*workloads.initial_noise(sim.shapes, w['noise'], w['seed']))
+        sim.step()                                    # warm-up (first-touch of the arrays)
+        t0 = time.perf_counter()
+        n = 0
+        while n < max_steps and (n < 2 or time.perf_counter() - t0 < steps_budget_s):
+            sim.step()
+            n += 1
+        dt = time.perf_counter() - t0
+    finally:
+        sim.close()
+    cells = w['settings']['nx'] * w['settings']['ny'] * w['settings']['nz']
+    return cells * n / dt, n, dt
+
+
+def reference_gpu_rate(workload, steps, warmup):
+    """The reference's own backend.cu (oracle/_ref build) on this GPU through its C ABI, wall clock."""
+    lib = ROOT / 'oracle' / '_ref' / 'libcavity_solver.so'
+    if not lib.is_file():
+        return None
+    from les_impulse3d_64_b200 import workloads
+    from les_impulse3d_64_b200.api import Solver
+    w = workloads.WORKLOADS[workload]
+    sim = Solver(w['settings'], library=lib)
+    try:
+        sim.initialize(*workloads.initial_noise(sim.shapes, w['noise'], w['seed']))
+        for _ in range(warmup):
+            sim.step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sim.step()
+        dt = time.perf_counter() - t0
+    finally:
+        sim.close()
+    cells = w['settings']['nx'] * w['settings']['ny'] * w['settings']['nz']
+    return {'value': cells * steps / dt, 'unit': 'cell-updates/s', 'steps': steps,
+            'what': "reference backend.cu built unchanged for sm_100a, driven through its C ABI, wall clock"}
+
+
+# ------------------------------------------------------------------------------------------ arms
+def run_ours(args, ranks):
+    from les_impulse3d_64_b200 import _build, workloads
+    from les_impulse3d_64_b200.api import Cavity, Solver
+    if ranks.rank == 0 and not _build.LIBRARY.is_file():
+        raise SystemExit('libcavity_solver.so is not built (python __graft_entry__.py)')
+    w = workloads.WORKLOADS[args.workload]
+    precision = args.precision or w.get('precision', 'fp64')
+    s = w['settings']
+    cells = s['nx'] * s['ny'] * s['nz']
+    field_bytes = 8 if precision == 'fp64' else 4
+
+    # device-timed steps
+    cav = Cavity(s, precision=precision)
+    cav.initialize(*workloads.initial_noise(cav.shapes, w['noise'], w['seed']))
+    passes0 = cav.pressure_passes()
+    ranks.barrier()
+    with ClockSampler() as clocks:
+        ms, kms = cav.time_steps(args.warmup, args.steps, flush_l2=True)
+    passes = cav.pressure_passes() - passes0
+    device_bytes = cav.device_bytes()
+    launches = args.steps * cav.kernels_per_step(0) + 7 * passes_in_timed(passes, args, cav)
+    cav.close()
+    total_ms = ranks.max(float(ms.sum()))
+    value = ranks.world * cells * args.steps / (total_ms / 1e3)
+
+    # end to end through the reference-facing ABI with host buffers
+    sim = Solver(s, precision=precision)
+    v, wn = workloads.initial_noise(sim.shapes, w['noise'], w['seed'])
+    sim.initialize(v, wn)
+    for _ in range(args.warmup):
+        sim.step()
+    ranks.barrier()
+    t0 = time.perf_counter()
+    sim.initialize(v, wn)
+    for _ in range(args.steps):
+        sim.step()
+        sim.probes()
+    fields = [sim.field(k) for k in ('u', 'v', 'w', 'mx', 'my', 'mz', 'phi')]
+    e2e_s = ranks.max(time.perf_counter() - t0)
+    sim.close()
+    h2d = (v.nbytes + wn.nbytes) / args.steps
+    d2h = 48 + 8 * s.get('n_probes', len(s['probes'])) + sum(f.nbytes for f in fields) / args.steps
+
+    peak, peak_kind = measured_peaks()
+    kernel_s = float(kms.sum()) / 1e3 / (3 * args.steps)
+    achieved = momentum_bytes(s, field_bytes) / kernel_s / 1e9
+    line = {
+        'metric': 'cell-updates/s per RK3 step', 'value': value, 'unit': 'cell-updates/s', 'n_gpus': ranks.world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64' if precision == 'fp64' else 'f32',
+        'data': 'synthetic (seeded Gaussian initial noise, numpy default_rng)',
+        'config': {'workload': args.workload, 'grid': [s['nx'], s['ny'], s['nz']], 'precision': precision,
+                   'stretch_beta': 1.5 if s.get('grid_stretch') else None, 're': round(1.0 / s['nu']),
+                   'l2': 'flushed before each timed step (256 MiB write)', 'parallelism': f'replicas x{ranks.world}',
+                   'device_bytes': device_bytes},
+        'e2e': {'value': ranks.world * cells * args.steps / e2e_s, 'unit': 'cell-updates/s',
+                'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
+        'gpu_launches': launches,
+        'pressure_passes_per_stage': passes / (3 * (args.steps + args.warmup)) if args.steps else None,
+        'roofline': {'kernel': 'momentum_kernel', 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                     'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
+                     'traffic': profile_traffic(args.workload), 'ms_per_launch': kernel_s * 1e3},
+        'clocks': clocks.summary(),
+    }
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
+        rate, n, dt = cpu_oracle_rate(args.workload)
+        line['cpu_baseline'] = {'value': rate, 'unit': 'cell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
+                                'sample': f'{n} steps of {args.workload} from its seeded initial state, {dt:.1f} s'}
+    return line
+
+
+def passes_in_timed(passes, args, cav):
+    # passes counted over warm-up + timed steps; scale to the timed steps
+    total = args.steps + args.warmup
+    return int(round(passes * args.steps / total)) if total else 0
+
+
+def run_reference(args, ranks):
+    if ranks.rank != 0:
+        return None
+    rate, n, dt = cpu_oracle_rate(args.workload, steps_budget_s=max(10.0, 2.0 * args.steps), max_steps=args.steps)
+    line = {
+        'metric': 'cell-updates/s per RK3 step', 'value': rate, 'unit': 'cell-updates/s', 'n_gpus': ranks.world,
+        'steps': n, 'warmup': 1, 'ms_per_step': dt / n * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded Gaussian initial noise, numpy default_rng)',
+        'config': {'workload': args.workload}, 'impl': 'reference',
+        'cpu_baseline': {'value': rate, 'unit': 'cell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
+                         'sample': f'{n} steps of {args.workload}, {dt:.1f} s (the reference ships no CPU path; '
+                                   'this is its FP64 OpenMP restatement)'},
+        'e2e': {'value': rate, 'unit': 'cell-updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    try:
+        ref = reference_gpu_rate(args.workload, args.steps, args.warmup)
+        if ref:
+            line['reference_binary_gpu'] = ref
+    except Exception as exc:          # the GPU reference build is an extra point, not the arm itself
+        line['reference_binary_gpu'] = {'unavailable': f'{type(exc).__name__}: {exc}'}
+    return line
+
+
+def main():
+    args = parse_args()
+    ranks = Ranks(args.gpus)
+    try:
+        line = run_ours(args, ranks) if args.impl == 'ours' else run_reference(args, ranks)
+        if line is not None and ranks.rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        ranks.close()
+
+
+if __name__ == '__main__':
+    main()

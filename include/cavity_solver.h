@@ -1,0 +1,107 @@
+/* cavity_solver.h - C ABI of the B200 cavity solver (libcavity_solver.so).
+ *
+ * Drop-in for the reference's ctypes boundary: the 18 `solver_*` functions below carry the names,
+ * arguments, return codes and record layouts of backend.cu:983-1195 (Config / Report / Diagnostics:
+ * backend.cu:584-597, mirrored by python_api.py:11-28).  Every function returns 0 on success and 1 on
+ * error, with the message in solver_last_error().  As in the reference, they act on one process-wide
+ * solver that solver_create replaces, every call is synchronous, and host buffers are caller-owned
+ * with sizes implied by the grid (u: (nx+1)*ny*nz, v: nx*(ny+1)*nz, w: nx*ny*(nz+1), phi: nx*ny*nz).
+ *
+ * The `cavity_*` functions after them are additions with no counterpart in the reference (the
+ * reference's solver is a singleton with one precision): a precision switch for the singleton and a
+ * handle API for several independent cavities in one process.
+ */
+#ifndef CAVITY_SOLVER_H
+#define CAVITY_SOLVER_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Solver settings; 288 bytes, first double at offset 48 (backend.cu:584-589). */
+typedef struct CavityConfig {
+    int nx, ny, nz, lid_shaped, impulse_order, adaptive_dt, dt_lag, phi_extrapolate, fdm_max_passes,
+        grid_stretch, n_probes;
+    double length, u_lid, nu, lz, lid_ramp_t, reinit_r, impulse_order4_ramp, grid_dx_wall, grid_max_aspect;
+    double dt_fixed, dt_max, cfl_target, diffusion_limit, fdm_rtol;
+    double probe_x[8], probe_y[8];
+} CavityConfig;
+
+/* Clock after a step; 48 bytes (backend.cu:590-594). dt_reason: 0 fixed, 1 DT_MAX, 2 CFL, 3 viscous. */
+typedef struct CavityReport {
+    long long steps;
+    double time, dt, cfl, phi_rel;
+    int dt_reason, phi_passes;
+} CavityReport;
+
+/* Volume-averaged diagnostics; 64 bytes (backend.cu:595-597). */
+typedef struct CavityDiagnostics {
+    double kinetic_energy, enstrophy, umax, div_rms, cfl_rate, gauge_ratio, gauge_x, gauge_y;
+} CavityDiagnostics;
+
+/* ---- the reference's boundary (backend.cu:1000-1195) ---- */
+int solver_create(const CavityConfig* config);                              /* backend.cu:1009 */
+int solver_initialize(const double* v_noise, const double* w_noise);        /* backend.cu:1075 */
+int solver_step(CavityReport* report);                                      /* backend.cu:1089 */
+int solver_kick(const double* nu, const double* nv, const double* nw, double amp, int passes); /* backend.cu:1092 */
+int solver_report(CavityReport* report);                                    /* backend.cu:1095 */
+int solver_diagnostics(CavityDiagnostics* d);                               /* backend.cu:1096 */
+int solver_grid(int axis, double* faces, double* centres);                  /* backend.cu:1131 */
+int solver_get_field(int field, void* out);                                 /* backend.cu:1139 */
+int solver_set_field(int field, const void* in);                            /* backend.cu:1147 */
+int solver_set_clock(double t, long long steps, double last_dt);            /* backend.cu:1156 */
+int solver_probes(float* out);                                              /* backend.cu:1159 */
+int solver_add_statistics(double weight, double* centreline);               /* backend.cu:1168 */
+int solver_get_statistics(double* sums);                                    /* backend.cu:1176 */
+int solver_set_statistics(const double* sums);                              /* backend.cu:1177 */
+int solver_midplane(float* out);                                            /* backend.cu:1178 */
+int solver_q_volume(int colour_w, float* q, float* colour);                 /* backend.cu:1185 */
+int solver_destroy(void);                                                   /* backend.cu:1000 */
+const char* solver_last_error(void);                                        /* backend.cu:1195 */
+
+/* ---- additions (no counterpart in the reference) ---- */
+/* Precision of the solver the next solver_create builds: 0 = FP64 fields (default), 1 = mixed (FP32
+ * fields, FP64 pressure).  Returns 1 for any other value. */
+int cavity_set_precision(int precision);
+
+/* The current field of the process-wide solver in double (velocity and impulse are float32 in
+ * solver_get_field); same numbering and sizes as solver_get_field. */
+int cavity_get_field_f64(int field, double* out);
+
+/* Handle API: several independent cavities.  A handle is an opaque pointer; the functions mirror the
+ * solver_* ones above with the handle as first argument. */
+typedef struct CavitySolver CavitySolver;
+int cavity_create(const CavityConfig* config, int precision, CavitySolver** out);
+int cavity_destroy(CavitySolver* s);
+int cavity_initialize(CavitySolver* s, const double* v_noise, const double* w_noise);
+int cavity_step(CavitySolver* s, CavityReport* report);
+/* Enqueue `count` steps without waiting for the GPU; cavity_sync then waits, checks every step's status
+ * and fills the report of the last one.  Steps of different handles overlap on the device. */
+int cavity_step_async(CavitySolver* s, int count);
+int cavity_sync(CavitySolver* s, CavityReport* report);
+int cavity_get_field(CavitySolver* s, int field, void* out);
+int cavity_set_field(CavitySolver* s, int field, const void* in);
+int cavity_probes(CavitySolver* s, float* out);
+int cavity_diagnostics(CavitySolver* s, CavityDiagnostics* d);
+/* Device bytes this cavity holds (state, work arrays, pressure tables), for admission control. */
+long long cavity_device_bytes(const CavitySolver* s);
+/* Bytes a cavity of this config would hold, without creating it. */
+long long cavity_estimate_bytes(const CavityConfig* config, int precision);
+
+/* Timing support for benchmarks: run `warmup` untimed steps, then `steps` steps, each bracketed by CUDA
+ * events on the solver's stream, with the L2 cache flushed (a 256 MiB device write) before each timed
+ * step when flush_l2 != 0.  ms_per_step[steps] receives each step's device time; kernel_ms[steps] (may be
+ * NULL) the device time of the momentum-sweep launches inside that step. */
+int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms_per_step, float* kernel_ms);
+/* The handle of the process-wide solver behind the solver_* functions (NULL if none). */
+CavitySolver* cavity_default(void);
+/* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */
+int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
+/* Pressure passes run by this cavity since it was created (all stages, steps and projections). */
+long long cavity_pressure_passes(const CavitySolver* s);
+const char* cavity_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

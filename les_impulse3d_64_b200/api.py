@@ -148,6 +148,12 @@ class Solver:
         self.call('solver_get_field', FIELD_NUMBER[name], pointer(out))
         return out
 
+    def field64(self, name):
+        """A field in double precision (an addition of the B200 build and the oracle)."""
+        out = np.empty(self.shapes[name], dtype=np.float64)
+        self.call('cavity_get_field_f64', FIELD_NUMBER[name], pointer(out))
+        return out
+
     def set_field(self, name, values):
         a = np.ascontiguousarray(values, dtype=np.float64 if name == 'phi' else np.float32)
         if a.shape != self.shapes[name]:
@@ -190,3 +196,108 @@ class Solver:
 
     def close(self):
         self.call('solver_destroy')
+
+
+class Cavity:
+    """Handle API of the B200 build (cavity_* functions): one of several independent cavities.
+
+    Same operations as `Solver` on an explicit handle, plus asynchronous stepping, device-memory
+    accounting and device-timed benchmark steps.
+    """
+
+    def __init__(self, settings, precision='fp64', library=None):
+        self.lib = load_library(library)
+        L = self.lib
+        L.cavity_create.argtypes = [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_void_p)]
+        for name in ('cavity_destroy', 'cavity_initialize', 'cavity_step', 'cavity_step_async', 'cavity_sync',
+                     'cavity_get_field', 'cavity_set_field', 'cavity_probes', 'cavity_diagnostics',
+                     'cavity_time_steps'):
+            getattr(L, name).restype = ct.c_int
+        L.cavity_destroy.argtypes = [ct.c_void_p]
+        L.cavity_initialize.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        L.cavity_step.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.cavity_step_async.argtypes = [ct.c_void_p, ct.c_int]
+        L.cavity_sync.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.cavity_get_field.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.cavity_set_field.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p]
+        L.cavity_probes.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.cavity_diagnostics.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.cavity_device_bytes.argtypes = [ct.c_void_p]
+        L.cavity_device_bytes.restype = ct.c_longlong
+        L.cavity_estimate_bytes.argtypes = [ct.c_void_p, ct.c_int]
+        L.cavity_estimate_bytes.restype = ct.c_longlong
+        L.cavity_time_steps.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p]
+        L.cavity_kernels_per_step.argtypes = [ct.c_void_p, ct.c_int]
+        L.cavity_pressure_passes.argtypes = [ct.c_void_p]
+        L.cavity_pressure_passes.restype = ct.c_longlong
+        L.cavity_last_error.restype = ct.c_char_p
+        self.config = make_config(settings)
+        nx, ny, nz = self.config.nx, self.config.ny, self.config.nz
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.n_cell = nx * ny * nz
+        self.shapes = {'u': (nz, ny, nx + 1), 'v': (nz, ny + 1, nx), 'w': (nz + 1, ny, nx), 'phi': (nz, ny, nx)}
+        self.shapes.update(mx=self.shapes['u'], my=self.shapes['v'], mz=self.shapes['w'])
+        self.handle = ct.c_void_p()
+        self._call('cavity_create', ct.byref(self.config), PRECISION[precision], ct.byref(self.handle))
+
+    def _call(self, name, *args):
+        if getattr(self.lib, name)(*args):
+            raise RuntimeError(self.lib.cavity_last_error().decode())
+
+    def initialize(self, v_noise=None, w_noise=None):
+        v = None if v_noise is None else np.ascontiguousarray(v_noise, dtype=np.float64)
+        w = None if w_noise is None else np.ascontiguousarray(w_noise, dtype=np.float64)
+        self._call('cavity_initialize', self.handle, pointer(v), pointer(w))
+
+    def step(self):
+        r = Report()
+        self._call('cavity_step', self.handle, ct.byref(r))
+        return Solver._as_dict(r)
+
+    def step_async(self, count=1):
+        self._call('cavity_step_async', self.handle, int(count))
+
+    def sync(self):
+        r = Report()
+        self._call('cavity_sync', self.handle, ct.byref(r))
+        return Solver._as_dict(r)
+
+    def field(self, name):
+        out = np.empty(self.shapes[name], dtype=np.float64 if name == 'phi' else np.float32)
+        self._call('cavity_get_field', self.handle, FIELD_NUMBER[name], pointer(out))
+        return out
+
+    def probes(self):
+        out = np.zeros(2 * self.config.n_probes, dtype=np.float32)
+        self._call('cavity_probes', self.handle, pointer(out))
+        return out
+
+    def device_bytes(self):
+        return int(self.lib.cavity_device_bytes(self.handle))
+
+    def kernels_per_step(self, passes_per_stage):
+        return int(self.lib.cavity_kernels_per_step(self.handle, int(passes_per_stage)))
+
+    def pressure_passes(self):
+        return int(self.lib.cavity_pressure_passes(self.handle))
+
+    def time_steps(self, warmup, steps, flush_l2=True):
+        """Device time (ms) of each of `steps` steps after `warmup`, and of its momentum-sweep launches."""
+        ms = np.zeros(steps, dtype=np.float32)
+        kms = np.zeros(steps, dtype=np.float32)
+        self._call('cavity_time_steps', self.handle, int(warmup), int(steps), int(bool(flush_l2)), pointer(ms),
+                   pointer(kms))
+        return ms, kms
+
+    def close(self):
+        if self.handle:
+            self._call('cavity_destroy', self.handle)
+            self.handle = ct.c_void_p()
+
+
+def estimate_bytes(settings, precision='fp64', library=None):
+    """Device bytes a cavity with these settings would hold (for admission against a memory budget)."""
+    lib = load_library(library)
+    lib.cavity_estimate_bytes.argtypes = [ct.c_void_p, ct.c_int]
+    lib.cavity_estimate_bytes.restype = ct.c_longlong
+    return int(lib.cavity_estimate_bytes(ct.byref(make_config(settings)), PRECISION[precision]))

@@ -1,0 +1,836 @@
+// solver.cu - host side of the B200 cavity solver and its C ABI (cavity_solver.h).
+//
+// One `Solver<T>` owns one cavity: its fields in HBM, a CUDA stream, and two instantiated CUDA graphs of a
+// whole time step (one per state parity, since the step writes the next state into the other buffer set).
+// A step is one graph launch: 1 + 3 x 4 kernels plus, per stage, a conditional while-node whose body is one
+// pressure pass (6 transform launches and a residual); the residual's last block decides on the device
+// whether another pass runs.  The host waits once per step, to read the 200-byte control block that holds
+// the clock, the report and any error.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cavity_solver.h"
+#include "kernels.cuh"
+#include "outputs.cuh"
+#include "setup.h"
+
+namespace cavity {
+
+[[noreturn]] static void fail(const std::string& m) { throw std::runtime_error(m); }
+static void check(cudaError_t e) {
+    if (e != cudaSuccess) fail(std::string("CUDA error: ") + cudaGetErrorString(e));
+}
+static unsigned int blocks_for(long long n) { return (unsigned int)((n + kThreads - 1) / kThreads); }
+
+// ------------------------------------------------------------------------------------------ device memory
+class DeviceArena {
+public:
+    ~DeviceArena() { release(); }
+    template <class T> T* alloc(long long n) {
+        void* p = nullptr;
+        const size_t bytes = sizeof(T) * (size_t)std::max(n, 1LL);
+        check(cudaMalloc(&p, bytes));
+        check(cudaMemset(p, 0, bytes));
+        ptrs_.push_back(p);
+        bytes_ += bytes;
+        return (T*)p;
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+        bytes_ = 0;
+    }
+    long long bytes() const { return bytes_; }
+private:
+    std::vector<void*> ptrs_;
+    long long bytes_ = 0;
+};
+
+class SolverBase {
+public:
+    virtual ~SolverBase() {}
+    virtual void initialize(const double* v, const double* w) = 0;
+    virtual void step_async(int count) = 0;
+    virtual void sync(CavityReport* r) = 0;
+    virtual void report(CavityReport* r) = 0;
+    virtual void kick(const double* const n[3], double amp, int passes) = 0;
+    virtual void diagnostics(CavityDiagnostics* d) = 0;
+    virtual void grid(int axis, double* faces, double* centres) = 0;
+    virtual void get_field(int field, void* out) = 0;
+    virtual void get_field_f64(int field, double* out) = 0;
+    virtual void set_field(int field, const void* in) = 0;
+    virtual void set_clock(double t, long long steps, double last_dt) = 0;
+    virtual void probes(float* out) = 0;
+    virtual void add_statistics(double weight, double* centreline) = 0;
+    virtual void get_statistics(double* sums) = 0;
+    virtual void set_statistics(const double* sums) = 0;
+    virtual void midplane(float* out) = 0;
+    virtual void q_volume(int colour_w, float* q, float* colour) = 0;
+    virtual long long device_bytes() const = 0;
+    virtual void time_steps(int warmup, int steps, int flush, float* ms, float* kms) = 0;
+    virtual int kernels_per_step(int passes) const = 0;
+    virtual long long pressure_passes() const = 0;
+    void step(CavityReport* r) {
+        step_async(1);
+        sync(r);
+    }
+};
+
+// ------------------------------------------------------------------------------------------ the solver
+template <class T> class Solver : public SolverBase {
+public:
+    explicit Solver(const CavityConfig& cfg) : c_(cfg) {
+        const std::string bad = check_config(c_);
+        if (!bad.empty()) fail(bad);
+        nx_ = c_.nx; ny_ = c_.ny; nz_ = c_.nz;
+        n_cell_ = (long long)nx_ * ny_ * nz_;
+        for (int k = 0; k < 3; k++) size_[k] = (long long)(nx_ + (k == 0)) * (ny_ + (k == 1)) * (nz_ + (k == 2));
+        max_face_ = std::max(size_[0], std::max(size_[1], size_[2]));
+        ax_[0] = make_axis_grid(c_, nx_, c_.length);
+        ax_[1] = make_axis_grid(c_, ny_, c_.length);
+        ax_[2] = make_axis_grid(c_, nz_, nz_ * (c_.lz / nz_));
+        volume_ = ax_[0].length * ax_[1].length * ax_[2].length;
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
+        setup_params();
+        allocate();
+        upload_tables();
+        build_graphs();
+        check(cudaStreamSynchronize(stream_));
+    }
+    ~Solver() override {
+        for (int s = 0; s < 2; s++) {
+            if (exec_[s]) cudaGraphExecDestroy(exec_[s]);
+            if (graph_[s]) cudaGraphDestroy(graph_[s]);
+            if (texec_[s]) cudaGraphExecDestroy(texec_[s]);
+            if (tgraph_[s]) cudaGraphDestroy(tgraph_[s]);
+        }
+        for (cudaEvent_t& e : kev_) if (e) cudaEventDestroy(e);
+        if (stream_) cudaStreamSynchronize(stream_);
+        arena_.release();
+        if (flush_) cudaFree(flush_);
+        if (stream_) cudaStreamDestroy(stream_);
+        if (body_stream_) cudaStreamDestroy(body_stream_);
+    }
+
+    // -------------------------------------------------------------------------------- ABI operations
+    void initialize(const double* v_noise, const double* w_noise) override {         // backend.cu:1075-1088
+        const double* src[3] = {nullptr, v_noise, w_noise};
+        for (int k = 0; k < 3; k++) {
+            if (src[k]) check(cudaMemcpyAsync(dstage_[0], src[k], sizeof(double) * size_[k], cudaMemcpyHostToDevice, stream_));
+            noise_to_field_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(src[k] ? dstage_[0] : nullptr, M_[par_][k], size_[k]);
+        }
+        T* m[3] = {M_[par_][0], M_[par_][1], M_[par_][2]};
+        T* u[3] = {U_[par_][0], U_[par_][1], U_[par_][2]};
+        project(m, PHI_[par_], u);
+        hc_.t = 0; hc_.steps = 0; hc_.last_dt = 0; hc_.hist_count = 0; hc_.have_prev = 0;
+        push_control();
+        check(cudaStreamSynchronize(stream_));
+    }
+
+    void step_async(int count) override {
+        if (pending_.empty()) steps_before_ = hc_.steps;
+        for (int i = 0; i < count; i++) {
+            check(cudaGraphLaunch(exec_[par_], stream_));
+            // the parity flips only when the step succeeds; sync() checks that for the queued steps
+            pending_.push_back(par_);
+            par_ ^= 1;
+        }
+    }
+    void sync(CavityReport* r) override {
+        check(cudaStreamSynchronize(stream_));
+        pull_control();
+        const size_t queued = pending_.size();
+        const std::vector<int> pending_copy = pending_;
+        pending_.clear();
+        if (hc_.error) {
+            // steps before the failed one committed; the failed step left the state buffers of its parity
+            // untouched and every later queued step skipped its work
+            const long long ok = hc_.steps - steps_before_;
+            par_ = (ok >= 0 && ok < (long long)queued) ? pending_copy[ok] : par_;
+            const int code = hc_.error;
+            hc_.error = kOk;
+            push_control();
+            check(cudaStreamSynchronize(stream_));
+            raise_error(code);
+        }
+        check(cudaGetLastError());
+        if (r) report(r);
+    }
+    void report(CavityReport* r) override {
+        r->steps = hc_.steps; r->time = hc_.t; r->dt = hc_.last_dt; r->cfl = hc_.last_cfl;
+        r->phi_rel = hc_.phi_rel; r->dt_reason = hc_.dt_reason; r->phi_passes = hc_.phi_passes;
+    }
+
+    void kick(const double* const noise[3], double amp, int passes) override {        // backend.cu:958-978
+        const int S = par_, X2 = par_ ^ 1;
+        for (int k = 0; k < 3; k++) {
+            const int sx = nx_ + (k == 0), sy = ny_ + (k == 1), sz = nz_ + (k == 2);
+            check(cudaMemcpyAsync(dstage_[0], noise[k], sizeof(double) * size_[k], cudaMemcpyHostToDevice, stream_));
+            double* a = dstage_[0];
+            double* b = dstage_[1];
+            for (int p = 0; p < std::max(1, passes); p++)
+                for (int axis = 2; axis >= 0; axis--) {
+                    smooth_kernel<<<blocks_for(size_[k]), kThreads, 0, stream_>>>(a, b, axis, sx, sy, sz);
+                    std::swap(a, b);
+                }
+            sumsq_kernel<<<blocks_for(size_[k]), kThreads, 0, stream_>>>(a, size_[k], slots_, partial_, out_counters_);
+            add_noise_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(U_[S][k], a, slots_, amp * c_.u_lid,
+                                                                               size_[k], M0_[k]);
+        }
+        // project the disturbed velocity (scratch potential; the state potential is unchanged)
+        T* tmp[3] = {M0_[0], M0_[1], M0_[2]};
+        T* nu[3] = {U_[X2][0], U_[X2][1], U_[X2][2]};
+        project(tmp, PHI_[2], nu);
+        for (int k = 0; k < 3; k++)
+            kick_update_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(M_[S][k], U_[S][k], U_[X2][k], size_[k]);
+        check(cudaStreamSynchronize(stream_));
+        check(cudaGetLastError());
+    }
+
+    void diagnostics(CavityDiagnostics* d) override {                                  // backend.cu:1096-1129
+        OutArgs<T> a = out_args();
+        const T lidv = (T)lid_speed_host(hc_.t);
+        cell_diag_kernel<T><<<blocks_for(n_cell_), kThreads, 0, stream_>>>(a, lidv);
+        for (int k = 0; k < 3; k++)
+            max_abs_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(a, k, size_[k], partial_ + 4 * partial_blocks_);
+        double slots[kNumSlots];
+        check(cudaMemcpyAsync(slots, slots_, sizeof slots, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+        d->kinetic_energy = slots[kSlotKE] / volume_;
+        d->enstrophy = 0.5 * slots[kSlotEns] / volume_;
+        d->div_rms = std::sqrt(slots[kSlotDiv2] / volume_);
+        double umax = 0;
+        for (int k = 0; k < 3; k++) umax = std::max(umax, slots[kSlotUmax0 + k]);
+        d->umax = umax;
+        d->cfl_rate = hc_.cfl_rate;
+        double best = -1;
+        int best_comp = 0;
+        long long best_i = 0;
+        for (int k = 0; k < 3; k++) {
+            const double val = slots[kSlotGauge0 + k];
+            if (val > best) { best = val; best_comp = k; best_i = (long long)slots[kSlotGaugeIdx0 + k]; }
+        }
+        const int sx = nx_ + (best_comp == 0), sy = ny_ + (best_comp == 1);
+        const int ix = (int)(best_i % sx), iy = (int)((best_i / sx) % sy);
+        d->gauge_ratio = best / std::max(umax, 1e-30);
+        d->gauge_x = (best_comp == 0 ? ax_[0].face[ix] : ax_[0].centre[std::min(ix, nx_ - 1)]) / c_.length;
+        d->gauge_y = (best_comp == 1 ? ax_[1].face[iy] : ax_[1].centre[std::min(iy, ny_ - 1)]) / c_.length;
+    }
+
+    void grid(int axis, double* faces, double* centres) override {
+        if (axis < 0 || axis > 2) fail("axis must be 0, 1 or 2");
+        std::copy(ax_[axis].face.begin(), ax_[axis].face.end(), faces);
+        std::copy(ax_[axis].centre.begin(), ax_[axis].centre.end(), centres);
+    }
+
+    void get_field(int field, void* out) override {                                   // backend.cu:1139-1146
+        if (field < 0 || field > 6) fail("field must be 0..6");
+        if (field == 6) {
+            check(cudaMemcpyAsync(out, PHI_[par_], sizeof(double) * n_cell_, cudaMemcpyDeviceToHost, stream_));
+        } else {
+            const int k = field % 3;
+            const T* src = field < 3 ? U_[par_][k] : M_[par_][k];
+            convert_kernel<T, float><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(src, fstage_, size_[k]);
+            check(cudaMemcpyAsync(out, fstage_, sizeof(float) * size_[k], cudaMemcpyDeviceToHost, stream_));
+        }
+        check(cudaStreamSynchronize(stream_));
+    }
+    void get_field_f64(int field, double* out) override {
+        if (field < 0 || field > 6) fail("field must be 0..6");
+        if (field == 6) {
+            check(cudaMemcpyAsync(out, PHI_[par_], sizeof(double) * n_cell_, cudaMemcpyDeviceToHost, stream_));
+        } else {
+            const int k = field % 3;
+            const T* src = field < 3 ? U_[par_][k] : M_[par_][k];
+            convert_kernel<T, double><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(src, dstage_[0], size_[k]);
+            check(cudaMemcpyAsync(out, dstage_[0], sizeof(double) * size_[k], cudaMemcpyDeviceToHost, stream_));
+        }
+        check(cudaStreamSynchronize(stream_));
+    }
+    void set_field(int field, const void* in) override {                              // backend.cu:1147-1155
+        if (field < 0 || field > 6) fail("field must be 0..6");
+        if (field == 6) {
+            check(cudaMemcpyAsync(PHI_[par_], in, sizeof(double) * n_cell_, cudaMemcpyHostToDevice, stream_));
+        } else {
+            const int k = field % 3;
+            T* dst = field < 3 ? U_[par_][k] : M_[par_][k];
+            check(cudaMemcpyAsync(fstage_, in, sizeof(float) * size_[k], cudaMemcpyHostToDevice, stream_));
+            convert_kernel<float, T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(fstage_, dst, size_[k]);
+        }
+        hc_.hist_count = 0;
+        hc_.have_prev = 0;
+        push_control();
+        update_cfl();
+        check(cudaStreamSynchronize(stream_));
+        pull_control();
+    }
+    void set_clock(double t, long long steps, double last_dt) override {
+        hc_.t = t; hc_.steps = steps; hc_.last_dt = last_dt;
+        push_control();
+        check(cudaStreamSynchronize(stream_));
+    }
+    void probes(float* out) override {                                                // backend.cu:1159-1166
+        if (c_.n_probes == 0) return;
+        probes_kernel<T><<<1, 32, 0, stream_>>>(out_args(), probe_cells_, c_.n_probes, probe_out_);
+        check(cudaMemcpyAsync(out, probe_out_, sizeof(float) * 2 * c_.n_probes, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    void add_statistics(double weight, double* centreline) override {                  // backend.cu:1168-1175
+        statistics_kernel<T><<<blocks_for((long long)nx_ * ny_ + nx_), kThreads, 0, stream_>>>(out_args(), weight, stats_, line_);
+        check(cudaMemcpyAsync(centreline, line_, sizeof(double) * 5 * nx_, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    void get_statistics(double* sums) override {
+        check(cudaMemcpyAsync(sums, stats_, sizeof(double) * 6 * nx_ * ny_, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    void set_statistics(const double* sums) override {
+        check(cudaMemcpyAsync(stats_, sums, sizeof(double) * 6 * nx_ * ny_, cudaMemcpyHostToDevice, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    void midplane(float* out) override {                                               // backend.cu:1178-1184
+        midplane_kernel<T><<<blocks_for((long long)nx_ * ny_), kThreads, 0, stream_>>>(out_args(), (T)lid_speed_host(hc_.t), plane_);
+        check(cudaMemcpyAsync(out, plane_, sizeof(float) * 4 * nx_ * ny_, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    void q_volume(int colour_w, float* q, float* colour) override {                    // backend.cu:1185-1194
+        const double L_over_U = c_.length / c_.u_lid;
+        float* qd = fstage_;
+        float* cd = fstage_ + n_cell_;
+        q_kernel<T><<<blocks_for(n_cell_), kThreads, 0, stream_>>>(out_args(), (T)lid_speed_host(hc_.t), (T)(L_over_U * L_over_U),
+                                                                  (T)(1.0 / c_.u_lid), colour_w, qd, cd);
+        check(cudaMemcpyAsync(q, qd, sizeof(float) * n_cell_, cudaMemcpyDeviceToHost, stream_));
+        check(cudaMemcpyAsync(colour, cd, sizeof(float) * n_cell_, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    long long device_bytes() const override { return arena_.bytes(); }
+
+    int kernels_per_step(int passes) const override { return 1 + 3 * 4 + 3 * passes * 7; }
+    long long pressure_passes() const override { return hc_.pass_count; }
+
+    void time_steps(int warmup, int steps, int flush, float* ms, float* kms) override {
+        if (flush && !flush_) check(cudaMalloc(&flush_, kFlushBytes));
+        for (int i = 0; i < warmup; i++) step(nullptr);
+        cudaEvent_t e0, e1;
+        check(cudaEventCreate(&e0));
+        check(cudaEventCreate(&e1));
+        for (int i = 0; i < steps; i++) {
+            if (flush) check(cudaMemsetAsync(flush_, i & 0xff, kFlushBytes, stream_));
+            check(cudaEventRecord(e0, stream_));
+            check(cudaGraphLaunch(texec_[par_], stream_));
+            pending_.push_back(par_);
+            par_ ^= 1;
+            check(cudaEventRecord(e1, stream_));
+            sync(nullptr);
+            check(cudaEventElapsedTime(&ms[i], e0, e1));
+            if (kms) {
+                float tot = 0, t;
+                for (int s = 0; s < 3; s++) {
+                    check(cudaEventElapsedTime(&t, kev_[2 * s], kev_[2 * s + 1]));
+                    tot += t;
+                }
+                kms[i] = tot;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+
+private:
+    static constexpr size_t kFlushBytes = 256ull << 20;
+
+    // ------------------------------------------------------------------------------ set-up
+    void setup_params() {
+        Params& p = p_;
+        p.nx = nx_; p.ny = ny_; p.nz = nz_; p.n_cell = (int)n_cell_;
+        p.o4 = c_.impulse_order == 4;
+        p.adaptive_dt = c_.adaptive_dt; p.dt_lag = c_.dt_lag; p.phi_extrapolate = c_.phi_extrapolate;
+        p.fdm_max_passes = c_.fdm_max_passes;
+        p.nu = c_.nu; p.u_lid = c_.u_lid; p.lid_ramp_t = c_.lid_ramp_t; p.reinit_r = c_.reinit_r;
+        p.dt_fixed = c_.dt_fixed; p.dt_max = c_.dt_max; p.cfl_target = c_.cfl_target;
+        p.diffusion_limit = c_.diffusion_limit; p.fdm_rtol = c_.fdm_rtol;
+        p.viscous_rate = (double)viscous_rate(c_, ax_);
+        std::memset(&hc_, 0, sizeof hc_);
+    }
+
+    void allocate() {
+        for (int s = 0; s < 3; s++) {
+            for (int k = 0; k < 3; k++) {
+                U_[s][k] = arena_.alloc<T>(size_[k]);
+                M_[s][k] = arena_.alloc<T>(size_[k]);
+            }
+            PHI_[s] = arena_.alloc<double>(n_cell_);
+        }
+        for (int k = 0; k < 3; k++) M0_[k] = arena_.alloc<T>(size_[k]);
+        phi0_ = arena_.alloc<double>(n_cell_);
+        base_ = arena_.alloc<double>(n_cell_);
+        rhs_ = arena_.alloc<double>(n_cell_);
+        res_ = arena_.alloc<double>(n_cell_);
+        for (int k = 0; k < 4; k++) hist_[k] = arena_.alloc<double>(n_cell_);
+        t1_ = arena_.alloc<double>(n_cell_);
+        t2_ = arena_.alloc<double>(n_cell_);
+        inv_lambda_ = arena_.alloc<double>(n_cell_);
+        partial_blocks_ = (long long)blocks_for(std::max(max_face_, n_cell_)) + 8;
+        partial_ = arena_.alloc<double>(8 * partial_blocks_);
+        ctrl_ = arena_.alloc<Control>(1);
+        slots_ = arena_.alloc<double>(kNumSlots);
+        out_counters_ = arena_.alloc<unsigned int>(kNumOutCounters);
+        stats_ = arena_.alloc<double>(6LL * nx_ * ny_);
+        line_ = arena_.alloc<double>(5LL * nx_);
+        plane_ = arena_.alloc<float>(4LL * nx_ * ny_);
+        fstage_ = arena_.alloc<float>(std::max(max_face_, 2 * n_cell_));
+        dstage_[0] = arena_.alloc<double>(max_face_);
+        dstage_[1] = arena_.alloc<double>(max_face_);
+        probe_cells_ = arena_.alloc<int>(24);
+        probe_out_ = arena_.alloc<float>(16);
+    }
+
+    void upload_tables() {
+        Geo<T>& g = geo_;
+        for (int a = 0; a < 3; a++) {
+            const AxisGrid& ag = ax_[a];
+            const int stride = ag.n + 2;
+            const std::vector<T> t = axis_tables<T>(ag, c_.impulse_order4_ramp, stride);
+            T* d = arena_.alloc<T>((long long)t.size());
+            check(cudaMemcpy(d, t.data(), sizeof(T) * t.size(), cudaMemcpyHostToDevice));
+            g.tab[a] = d;
+            g.stride[a] = stride;
+            std::vector<double> inv(ag.n + 1);
+            for (int i = 0; i <= ag.n; i++) inv[i] = 1.0 / ag.spacing[i];
+            double* dw = arena_.alloc<double>(ag.n);
+            double* di = arena_.alloc<double>(ag.n + 1);
+            check(cudaMemcpy(dw, ag.width.data(), sizeof(double) * ag.n, cudaMemcpyHostToDevice));
+            check(cudaMemcpy(di, inv.data(), sizeof(double) * (ag.n + 1), cudaMemcpyHostToDevice));
+            g.dw[a] = dw;
+            g.dinv_sp[a] = di;
+            double* cen = arena_.alloc<double>(ag.n);
+            check(cudaMemcpy(cen, ag.centre.data(), sizeof(double) * ag.n, cudaMemcpyHostToDevice));
+            centre_[a] = cen;
+        }
+        const std::vector<T> lid = lid_u_table<T>(c_, ax_);
+        T* dl = arena_.alloc<T>((long long)lid.size());
+        check(cudaMemcpy(dl, lid.data(), sizeof(T) * lid.size(), cudaMemcpyHostToDevice));
+        g.lid_u = dl;
+        // pressure eigenbases (FP64) and 1/(lambda_x + lambda_y + lambda_z), 0 at the constant mode
+        AxisEigen e[3];
+        for (int a = 0; a < 3; a++) {
+            e[a] = axis_eigen(ax_[a]);
+            const int n = ax_[a].n;
+            std::vector<double> st((size_t)n * n);
+            for (int i = 0; i < n; i++)
+                for (int j = 0; j < n; j++) st[(size_t)j * n + i] = e[a].S[(size_t)i * n + j];
+            S_[a] = arena_.alloc<double>((long long)n * n);
+            ST_[a] = arena_.alloc<double>((long long)n * n);
+            check(cudaMemcpy(S_[a], e[a].S.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice));
+            check(cudaMemcpy(ST_[a], st.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice));
+        }
+        std::vector<double> inv((size_t)n_cell_);
+        for (int z = 0; z < nz_; z++)
+            for (int y = 0; y < ny_; y++)
+                for (int x = 0; x < nx_; x++) {
+                    const bool zero = x == e[0].zero_mode && y == e[1].zero_mode && z == e[2].zero_mode;
+                    inv[x + (size_t)nx_ * (y + (size_t)ny_ * z)] =
+                        zero ? 0.0 : 1.0 / (e[2].lambda[z] + e[1].lambda[y] + e[0].lambda[x]);
+                }
+        check(cudaMemcpy(inv_lambda_, inv.data(), sizeof(double) * n_cell_, cudaMemcpyHostToDevice));
+        const std::vector<int> cells = probe_cells(c_, ax_);
+        if (!cells.empty()) check(cudaMemcpy(probe_cells_, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+        push_control();
+    }
+
+    double lid_speed_host(double time) const {
+        if (c_.lid_ramp_t > 0) return c_.u_lid * std::min(1.0, std::max(time, 0.0) / c_.lid_ramp_t);
+        return c_.u_lid;
+    }
+
+    void push_control() { check(cudaMemcpyAsync(ctrl_, &hc_, sizeof hc_, cudaMemcpyHostToDevice, stream_)); }
+    void pull_control() {
+        check(cudaMemcpyAsync(&hc_, ctrl_, sizeof hc_, cudaMemcpyDeviceToHost, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+
+    [[noreturn]] void raise_error(int code) {
+        char msg[200];
+        switch (code) {
+        case kVelocityNaN: fail("velocity is NaN/inf: the solution has blown up");
+        case kRhsNaN: fail("pressure solve: right-hand side is NaN/inf (the run has blown up)");
+        case kResidualNaN: fail("pressure solve: residual is NaN/inf");
+        case kNotConverged:
+            std::snprintf(msg, sizeof msg, "pressure solve: residual %.2e > FDM_RTOL after %d passes", hc_.error_value,
+                          hc_.error_passes);
+            fail(msg);
+        default: fail("solver error " + std::to_string(code));
+        }
+    }
+
+    OutArgs<T> out_args() const {
+        OutArgs<T> a;
+        a.p = p_;
+        a.g = geo_;
+        for (int k = 0; k < 3; k++) { a.u[k] = U_[par_][k]; a.m[k] = M_[par_][k]; }
+        a.centre_x = centre_[0];
+        a.centre_z = centre_[2];
+        a.length_x = (double)(float)ax_[0].length;
+        a.length_z = (double)(float)ax_[2].length;
+        a.lid_shaped = c_.lid_shaped;
+        a.slots = slots_;
+        a.partial = partial_;
+        a.counters = out_counters_;
+        return a;
+    }
+
+    void update_cfl() {
+        CflArgs<T> a;
+        a.p = p_;
+        a.g = geo_;
+        for (int k = 0; k < 3; k++) a.u[k] = U_[par_][k];
+        a.c = ctrl_;
+        a.partial = partial_;
+        cfl_kernel<T><<<blocks_for(n_cell_), kThreads, 0, stream_>>>(a);
+    }
+
+    // ------------------------------------------------------------------------------ kernel launches
+    void launch_momentum(cudaStream_t st, int stage, int S, int in, int out) {
+        MomentumArgs<T> a;
+        a.p = p_;
+        a.g = geo_;
+        for (int k = 0; k < 3; k++) {
+            a.u[k] = U_[in][k];
+            a.m[k] = M_[stage == 0 ? S : in][k];
+            a.m0[k] = M0_[k];
+            a.m0_out[k] = M0_[k];
+            a.out[k] = M_[out][k];
+        }
+        a.c = ctrl_;
+        a.stage = stage;
+        a.r = (T)c_.reinit_r;
+        a.one_minus_r = (T)(1.0 - c_.reinit_r);
+        a.nu = (T)c_.nu;
+        dim3 grid(blocks_for(max_face_), 3);
+        momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
+    }
+    void launch_divergence(cudaStream_t st, T* const m[3], bool step_mode, int stage, int S, int cur, int out) {
+        DivergenceArgs<T> a;
+        a.p = p_;
+        a.g = geo_;
+        for (int k = 0; k < 3; k++) a.m[k] = m[k];
+        a.rhs = rhs_;
+        a.phi_state = PHI_[S];
+        a.phi0 = phi0_;
+        a.phi_cur = PHI_[cur];
+        a.base = step_mode ? base_ : nullptr;
+        a.guess = PHI_[out];
+        for (int k = 0; k < 4; k++) a.hist[k] = hist_[k];
+        a.stage = stage;
+        a.c = ctrl_;
+        a.partial = partial_;
+        divergence_kernel<T><<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
+    }
+    void launch_residual(cudaStream_t st, double* phi, bool first, bool have_guess, cudaGraphConditionalHandle h, bool use_h) {
+        ResidualArgs a;
+        a.p = p_;
+        for (int k = 0; k < 3; k++) { a.dw[k] = geo_.dw[k]; a.dinv_sp[k] = geo_.dinv_sp[k]; }
+        a.phi = phi;
+        a.rhs = rhs_;
+        a.res = res_;
+        a.first = first;
+        a.have_guess = have_guess;
+        a.c = ctrl_;
+        a.partial = partial_;
+        a.handle = h;
+        a.use_handle = use_h;
+        residual_kernel<<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
+    }
+    template <int BM, int BN, int BK, int TM, int TN>
+    void gemm(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda, long long sA,
+              const double* B, int ldb, long long sB, double* C, int ldc, long long sC, int batch, int epi, double* phi,
+              cudaGraphConditionalHandle h = 0, bool clear = false) {
+        GemmArgs<double> g;
+        g.handle = h;
+        g.clear_condition = clear;
+        g.M = M; g.N = N; g.K = K; g.lda = lda; g.ldb = ldb; g.ldc = ldc;
+        g.sA = sA; g.sB = sB; g.sC = sC;
+        g.A = A; g.A_alt = A_alt; g.B = B; g.C = C;
+        g.inv_lambda = inv_lambda_;
+        g.phi = phi;
+        g.epilogue = epi;
+        g.c = ctrl_;
+        dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch);
+        gemm_kernel<double, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(g);
+    }
+    // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
+    void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
+        const int plane = nx_ * ny_;
+        const long long pl = plane;
+        gemm<32, 32, 8, 2, 2>(st, ny_ * nz_, nx_, nx_, res_, rhs_, nx_, 0, S_[0], nx_, 0, t1_, nx_, 0, 1, kStore, nullptr,
+                              h, use_h);
+        gemm<32, 32, 8, 2, 2>(st, ny_, nx_, ny_, ST_[1], nullptr, ny_, 0, t1_, nx_, pl, t2_, nx_, pl, nz_, kStore, nullptr);
+        gemm<32, 32, 8, 2, 2>(st, nz_, plane, nz_, ST_[2], nullptr, nz_, 0, t2_, plane, 0, t1_, plane, 0, 1, kScaleInvLambda, nullptr);
+        gemm<32, 32, 8, 2, 2>(st, nz_, plane, nz_, S_[2], nullptr, nz_, 0, t1_, plane, 0, t2_, plane, 0, 1, kStore, nullptr);
+        gemm<32, 32, 8, 2, 2>(st, ny_, nx_, ny_, S_[1], nullptr, ny_, 0, t2_, nx_, pl, t1_, nx_, pl, nz_, kStore, nullptr);
+        gemm<32, 32, 8, 2, 2>(st, ny_ * nz_, nx_, nx_, t1_, nullptr, nx_, 0, ST_[0], nx_, 0, nullptr, nx_, 0, 1, kAccumulate, phi);
+        launch_residual(st, phi, false, true, h, use_h);
+    }
+    void launch_finish(cudaStream_t st, T* const m[3], T* const u_out[3], double* phi, bool step_mode, int stage, bool last) {
+        FinishArgs<T> a;
+        a.p = p_;
+        a.g = geo_;
+        for (int k = 0; k < 3; k++) { a.m[k] = m[k]; a.u_out[k] = u_out[k]; }
+        a.phi = phi;
+        a.base = base_;
+        for (int k = 0; k < 4; k++) a.hist[k] = hist_[k];
+        a.step_mode = step_mode;
+        a.last_stage = last;
+        a.stage = stage;
+        a.c = ctrl_;
+        a.partial = partial_;
+        finish_kernel<T><<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
+    }
+
+    // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
+    // `first_residual` launches the kernel that sets the loop condition before the node.
+    template <class F>
+    void captured_loop(F first_residual, double* phi) {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g;
+        const cudaGraphNode_t* deps;
+        size_t ndeps;
+        check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
+        cudaGraphConditionalHandle h;
+        check(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+        first_residual(h);
+        check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        check(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        check(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        launch_pass(body_stream_, phi, h, true);
+        check(cudaStreamEndCapture(body_stream_, &body));
+        check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+    }
+
+    // The time step for state parity S (backend.cu:877-955), enqueued on stream_ under capture.
+    void capture_step(int S, bool timing) {
+        const int Xs = S ^ 1, Ys = 2;
+        step_begin_kernel<<<1, 32, 0, stream_>>>(p_, ctrl_);
+        for (int stage = 0; stage < 3; stage++) {
+            const int in = stage == 0 ? S : stage == 1 ? Xs : Ys;
+            const int out = stage == 1 ? Ys : Xs;
+            const int cur = stage == 1 ? Xs : Ys;          // potential of the previous stage (stages 1, 2)
+            if (timing) check(cudaEventRecordWithFlags(kev_[2 * stage], stream_, cudaEventRecordExternal));
+            launch_momentum(stream_, stage, S, in, out);
+            if (timing) check(cudaEventRecordWithFlags(kev_[2 * stage + 1], stream_, cudaEventRecordExternal));
+            launch_divergence(stream_, M_[out], true, stage, S, cur, out);
+            double* phi = PHI_[out];
+            captured_loop([&](cudaGraphConditionalHandle h) { launch_residual(stream_, phi, true, true, h, true); }, phi);
+            launch_finish(stream_, M_[out], U_[out], phi, true, stage, stage == 2);
+        }
+    }
+
+    void build_graphs() {
+        for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
+        for (int S = 0; S < 2; S++)
+            for (int timing = 0; timing < 2; timing++) {
+                cudaGraph_t& g = timing ? tgraph_[S] : graph_[S];
+                cudaGraphExec_t& ex = timing ? texec_[S] : exec_[S];
+                check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+                capture_step(S, timing);
+                check(cudaStreamEndCapture(stream_, &g));
+                check(cudaGraphInstantiate(&ex, g, 0));
+            }
+    }
+
+    // A projection outside a step (initialize, kick): m -> u, phi from no guess (backend.cu:849-854), with
+    // the refinement loop driven from the host.  Also refreshes the CFL rate of u.
+    void project(T* const m[3], double* phi, T* const u_out[3]) {
+        hc_.error = kOk;
+        push_control();
+        for (int k = 0; k < 3; k++) zero_walls_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(p_, k, m[k]);
+        launch_divergence(stream_, m, false, 0, par_, par_, par_);
+        launch_residual(stream_, phi, true, false, 0, false);
+        pull_control();
+        int guard = 0;
+        while (hc_.cond && !hc_.error && guard++ < 1000) {
+            launch_pass(stream_, phi, 0, false);
+            pull_control();
+        }
+        if (hc_.error) {
+            const int code = hc_.error;
+            hc_.error = kOk;
+            push_control();
+            check(cudaStreamSynchronize(stream_));
+            raise_error(code);
+        }
+        launch_finish(stream_, m, u_out, phi, false, 0, true);
+        pull_control();
+    }
+
+    CavityConfig c_;
+    int nx_, ny_, nz_;
+    long long n_cell_, size_[3], max_face_;
+    AxisGrid ax_[3];
+    double volume_;
+    Params p_;
+    Geo<T> geo_;
+    Control hc_;
+    DeviceArena arena_;
+    cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
+    int par_ = 0;
+    std::vector<int> pending_;
+    long long steps_before_ = 0;
+    // fields: three buffer sets of velocity, impulse and potential (state, stage outputs)
+    T* U_[3][3];
+    T* M_[3][3];
+    double* PHI_[3];
+    T* M0_[3];
+    double *phi0_, *base_, *rhs_, *res_, *hist_[4], *t1_, *t2_, *inv_lambda_;
+    double *S_[3], *ST_[3];
+    double* partial_;
+    long long partial_blocks_;
+    Control* ctrl_;
+    double *slots_, *stats_, *line_, *dstage_[2];
+    unsigned int* out_counters_;
+    float *plane_, *fstage_, *probe_out_;
+    int* probe_cells_;
+    const double* centre_[3];
+    cudaGraph_t graph_[2] = {nullptr, nullptr}, tgraph_[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec_[2] = {nullptr, nullptr}, texec_[2] = {nullptr, nullptr};
+    cudaEvent_t kev_[6] = {};
+    void* flush_ = nullptr;
+};
+
+static SolverBase* make_solver(const CavityConfig& c, int precision) {
+    if (precision == 0) return new Solver<double>(c);
+    if (precision == 1) return new Solver<float>(c);
+    fail("precision must be 0 (fp64) or 1 (mixed)");
+}
+
+// bytes a cavity would hold: 3 sets x (3 face arrays x 2) + m0 of T, 14 cell arrays of double, tables
+static long long estimate_bytes(const CavityConfig& c, int precision) {
+    const long long nx = c.nx, ny = c.ny, nz = c.nz, cells = nx * ny * nz;
+    const long long faces = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1);
+    const long long fb = precision == 0 ? 8 : 4;
+    const long long maxface = std::max((nx + 1) * ny * nz, nx * ny * (nz + 1));
+    return 7 * faces * fb + 16 * cells * 8 + 2 * 8 * maxface + 4 * std::max(maxface, 2 * cells) +
+           2 * 8 * (nx * nx + ny * ny + nz * nz) + 64 * (maxface / 256 + 8) + (1 << 20);
+}
+
+}  // namespace cavity
+
+// ================================================================================================ C ABI
+using cavity::SolverBase;
+struct CavitySolver { std::unique_ptr<SolverBase> s; };
+
+static std::string g_last_error;
+static CavitySolver* g_default = nullptr;
+static int g_precision = 0;
+
+template <class F> static int safely(F f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return 1;
+    }
+}
+static SolverBase& S() {
+    if (!g_default) cavity::fail("no solver: call solver_create first");
+    return *g_default->s;
+}
+static SolverBase& H(CavitySolver* h) {
+    if (!h || !h->s) cavity::fail("invalid solver handle");
+    return *h->s;
+}
+
+extern "C" {
+int solver_destroy(void) {
+    return safely([&] {
+        delete g_default;
+        g_default = nullptr;
+    });
+}
+int solver_create(const CavityConfig* config) {
+    return safely([&] {
+        delete g_default;
+        g_default = nullptr;
+        std::unique_ptr<CavitySolver> h(new CavitySolver);
+        h->s.reset(cavity::make_solver(*config, g_precision));
+        g_default = h.release();
+    });
+}
+int solver_initialize(const double* v, const double* w) { return safely([&] { S().initialize(v, w); }); }
+int solver_step(CavityReport* r) { return safely([&] { S().step(r); }); }
+int solver_kick(const double* nu, const double* nv, const double* nw, double amp, int passes) {
+    return safely([&] { const double* n[3] = {nu, nv, nw}; S().kick(n, amp, passes); });
+}
+int solver_report(CavityReport* r) { return safely([&] { S().report(r); }); }
+int solver_diagnostics(CavityDiagnostics* d) { return safely([&] { S().diagnostics(d); }); }
+int solver_grid(int axis, double* faces, double* centres) { return safely([&] { S().grid(axis, faces, centres); }); }
+int solver_get_field(int field, void* out) { return safely([&] { S().get_field(field, out); }); }
+int solver_set_field(int field, const void* in) { return safely([&] { S().set_field(field, in); }); }
+int solver_set_clock(double t, long long steps, double last_dt) { return safely([&] { S().set_clock(t, steps, last_dt); }); }
+int solver_probes(float* out) { return safely([&] { S().probes(out); }); }
+int solver_add_statistics(double weight, double* centreline) { return safely([&] { S().add_statistics(weight, centreline); }); }
+int solver_get_statistics(double* sums) { return safely([&] { S().get_statistics(sums); }); }
+int solver_set_statistics(const double* sums) { return safely([&] { S().set_statistics(sums); }); }
+int solver_midplane(float* out) { return safely([&] { S().midplane(out); }); }
+int solver_q_volume(int colour_w, float* q, float* colour) { return safely([&] { S().q_volume(colour_w, q, colour); }); }
+const char* solver_last_error(void) { return g_last_error.c_str(); }
+
+int cavity_get_field_f64(int field, double* out) { return safely([&] { S().get_field_f64(field, out); }); }
+int cavity_set_precision(int precision) {
+    return safely([&] {
+        if (precision != 0 && precision != 1) cavity::fail("precision must be 0 (fp64) or 1 (mixed)");
+        g_precision = precision;
+    });
+}
+int cavity_create(const CavityConfig* config, int precision, CavitySolver** out) {
+    return safely([&] {
+        std::unique_ptr<CavitySolver> h(new CavitySolver);
+        h->s.reset(cavity::make_solver(*config, precision));
+        *out = h.release();
+    });
+}
+int cavity_destroy(CavitySolver* s) {
+    return safely([&] {
+        if (s == g_default) g_default = nullptr;
+        delete s;
+    });
+}
+int cavity_initialize(CavitySolver* s, const double* v, const double* w) { return safely([&] { H(s).initialize(v, w); }); }
+int cavity_step(CavitySolver* s, CavityReport* r) { return safely([&] { H(s).step(r); }); }
+int cavity_step_async(CavitySolver* s, int count) { return safely([&] { H(s).step_async(count); }); }
+int cavity_sync(CavitySolver* s, CavityReport* r) { return safely([&] { H(s).sync(r); }); }
+int cavity_get_field(CavitySolver* s, int field, void* out) { return safely([&] { H(s).get_field(field, out); }); }
+int cavity_set_field(CavitySolver* s, int field, const void* in) { return safely([&] { H(s).set_field(field, in); }); }
+int cavity_probes(CavitySolver* s, float* out) { return safely([&] { H(s).probes(out); }); }
+int cavity_diagnostics(CavitySolver* s, CavityDiagnostics* d) { return safely([&] { H(s).diagnostics(d); }); }
+long long cavity_device_bytes(const CavitySolver* s) { return s && s->s ? s->s->device_bytes() : -1; }
+long long cavity_estimate_bytes(const CavityConfig* config, int precision) {
+    return cavity::estimate_bytes(*config, precision);
+}
+int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms, float* kms) {
+    return safely([&] { H(s).time_steps(warmup, steps, flush_l2, ms, kms); });
+}
+CavitySolver* cavity_default(void) { return g_default; }
+int cavity_kernels_per_step(const CavitySolver* s, int passes) { return s && s->s ? s->s->kernels_per_step(passes) : -1; }
+long long cavity_pressure_passes(const CavitySolver* s) { return s && s->s ? s->s->pressure_passes() : -1; }
+const char* cavity_last_error(void) { return g_last_error.c_str(); }
+}

@@ -998,4 +998,13 @@ int solver_q_volume(int colour_w, float* q, float* colour) {                    
     });
 }
 const char* solver_last_error() { return last_error.c_str(); }
+// test-side addition: the fields in double (velocity and impulse are float32 in the reference ABI)
+int cavity_get_field_f64(int field, double* out) {
+    return safely([&] {
+        Oracle& s = S();
+        if (field < 3) for (long long i = 0; i < s.size[field]; i++) out[i] = (double)s.u[field][i];
+        else if (field < 6) for (long long i = 0; i < s.size[field - 3]; i++) out[i] = (double)s.m[field - 3][i];
+        else std::copy(s.phi.begin(), s.phi.end(), out);
+    });
+}
 }

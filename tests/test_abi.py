@@ -1,0 +1,59 @@
+"""The C ABI without a GPU: every symbol include/cavity_solver.h declares is exported by the built library,
+the record layouts match the reference's (byte sizes and offsets), and calls without a solver fail cleanly."""
+import ctypes as ct
+import re
+from pathlib import Path
+
+import pytest
+
+from les_impulse3d_64_b200 import _build
+from les_impulse3d_64_b200.api import Config, Diagnostics, Report, load_library
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / 'include' / 'cavity_solver.h'
+
+
+def declared_functions():
+    text = re.sub(r'/\*.*?\*/', '', HEADER.read_text(), flags=re.S)
+    names = re.findall(r'\b((?:solver|cavity)_[a-z0-9_]+)\s*\(', text)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope='module')
+def lib():
+    _build.build()
+    return load_library()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len([n for n in names if n.startswith('solver_')]) == 18
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert missing == []
+
+
+def test_record_layouts():
+    assert ct.sizeof(Config) == 288 and Config.length.offset == 48
+    assert ct.sizeof(Report) == 48 and ct.sizeof(Diagnostics) == 64
+
+
+def test_layouts_match_reference_binding():
+    """The reference's own python_api records, where its checkout is present."""
+    import importlib.util
+    src = Path('/root/reference/python_api.py')
+    if not src.is_file():
+        pytest.skip('reference checkout not present')
+    spec = importlib.util.spec_from_file_location('reference_python_api', src)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    for ours, theirs in ((Config, mod.Config), (Report, mod.Report), (Diagnostics, mod.Diagnostics)):
+        assert ct.sizeof(ours) == ct.sizeof(theirs)
+        assert [(n, getattr(ours, n).offset) for n, _ in ours._fields_] == \
+               [(n, getattr(theirs, n).offset) for n, _ in theirs._fields_]
+
+
+def test_calls_without_solver_fail_with_message(lib):
+    r = Report()
+    assert lib.solver_report(ct.byref(r)) == 1
+    assert lib.solver_last_error() == b'no solver: call solver_create first'
+    assert lib.solver_destroy() == 0
