@@ -34,7 +34,7 @@ sys.path.insert(0, str(ROOT))
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=30)
+    ap.add_argument('--steps', type=int, default=50)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
     ap.add_argument('--workload', default='c2_64cube_re1000')
@@ -81,56 +81,50 @@ class Ranks:
 
 # ------------------------------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
-    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
-             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
-             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+    """SM clock and clock-event (throttle) reasons sampled through NVML every 2 ms during the timed region."""
+    REASONS = {0x4: 'sw_power_cap', 0x8: 'hw_slowdown', 0x20: 'sw_thermal_slowdown', 0x40: 'hw_thermal_slowdown',
+               0x80: 'hw_power_brake_slowdown'}
 
-    def __init__(self, index=0):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, index=0, period=0.002):
+        self.index, self.period = index, period
+        self.samples, self.max_mhz, self.reasons = [], None, set()
+        self._stop = threading.Event()
+        self.nvml = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.QUERY}',
-                                          '--format=csv,noheader,nounits', '-lms', '100'],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            self.nvml = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                for bit, name in self.REASONS.items():
+                    if bits & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self.nvml:
+            self._stop.set()
+            self.thread.join(timeout=2)
 
     def summary(self):
-        mhz, max_mhz, reasons = [], None, set()
-        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
-        for line in self.lines:
-            f = [x.strip() for x in line.split(',')]
-            if len(f) < 9:
-                continue
-            try:
-                mhz.append(float(f[1]))
-                max_mhz = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower() == 'active':
-                    reasons.add(name)
-        return {'sm_mhz': statistics.median(mhz) if mhz else None, 'sm_max_mhz': max_mhz,
-                'reasons': sorted(reasons), 'samples': len(mhz)}
+        return {'sm_mhz': statistics.median(self.samples) if self.samples else None, 'sm_max_mhz': self.max_mhz,
+                'reasons': sorted(self.reasons), 'samples': len(self.samples)}
 
 
 # ------------------------------------------------------------------------------------------ helpers
@@ -226,7 +220,7 @@ def run_ours(args, ranks):
     cav.initialize(*workloads.initial_noise(cav.shapes, w['noise'], w['seed']))
     passes0 = cav.pressure_passes()
     ranks.barrier()
-    with ClockSampler() as clocks:
+    with ClockSampler(ranks.local) as clocks:
         ms, kms = cav.time_steps(args.warmup, args.steps, flush_l2=True)
     passes = cav.pressure_passes() - passes0
     device_bytes = cav.device_bytes()

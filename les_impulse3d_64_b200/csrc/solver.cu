@@ -141,7 +141,8 @@ public:
     void step_async(int count) override {
         if (pending_.empty()) steps_before_ = hc_.steps;
         for (int i = 0; i < count; i++) {
-            check(cudaGraphLaunch(exec_[par_], stream_));
+            if (eager_) enqueue_step(par_, false, true);
+            else check(cudaGraphLaunch(exec_[par_], stream_));
             // the parity flips only when the step succeeds; sync() checks that for the queued steps
             pending_.push_back(par_);
             par_ ^= 1;
@@ -328,7 +329,8 @@ public:
         for (int i = 0; i < steps; i++) {
             if (flush) check(cudaMemsetAsync(flush_, i & 0xff, kFlushBytes, stream_));
             check(cudaEventRecord(e0, stream_));
-            check(cudaGraphLaunch(texec_[par_], stream_));
+            if (eager_) enqueue_step(par_, true, true);
+            else check(cudaGraphLaunch(texec_[par_], stream_));
             pending_.push_back(par_);
             par_ ^= 1;
             check(cudaEventRecord(e1, stream_));
@@ -625,32 +627,51 @@ private:
         check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
     }
 
-    // The time step for state parity S (backend.cu:877-955), enqueued on stream_ under capture.
-    void capture_step(int S, bool timing) {
+    // The time step for state parity S (backend.cu:877-955), enqueued on stream_: under stream capture (the
+    // refinement loops become conditional while-nodes), or eagerly with the loops driven from the host (the
+    // launch mode for profilers, which cannot see kernels inside graphs that hold conditional nodes).
+    void enqueue_step(int S, bool timing, bool eager) {
         const int Xs = S ^ 1, Ys = 2;
+        auto mark = [&](cudaEvent_t e) {
+            if (eager) check(cudaEventRecord(e, stream_));
+            else check(cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal));
+        };
         step_begin_kernel<<<1, 32, 0, stream_>>>(p_, ctrl_);
         for (int stage = 0; stage < 3; stage++) {
             const int in = stage == 0 ? S : stage == 1 ? Xs : Ys;
             const int out = stage == 1 ? Ys : Xs;
             const int cur = stage == 1 ? Xs : Ys;          // potential of the previous stage (stages 1, 2)
-            if (timing) check(cudaEventRecordWithFlags(kev_[2 * stage], stream_, cudaEventRecordExternal));
+            if (timing) mark(kev_[2 * stage]);
             launch_momentum(stream_, stage, S, in, out);
-            if (timing) check(cudaEventRecordWithFlags(kev_[2 * stage + 1], stream_, cudaEventRecordExternal));
+            if (timing) mark(kev_[2 * stage + 1]);
             launch_divergence(stream_, M_[out], true, stage, S, cur, out);
             double* phi = PHI_[out];
-            captured_loop([&](cudaGraphConditionalHandle h) { launch_residual(stream_, phi, true, true, h, true); }, phi);
+            if (eager) {
+                launch_residual(stream_, phi, true, true, 0, false);
+                pull_control();
+                while (hc_.cond && !hc_.error) {
+                    launch_pass(stream_, phi, 0, false);
+                    pull_control();
+                }
+            } else {
+                captured_loop([&](cudaGraphConditionalHandle h) { launch_residual(stream_, phi, true, true, h, true); },
+                              phi);
+            }
             launch_finish(stream_, M_[out], U_[out], phi, true, stage, stage == 2);
         }
     }
 
     void build_graphs() {
         for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
+        const char* env = std::getenv("CAVITY_GRAPHS");
+        eager_ = env && env[0] == '0';
+        if (eager_) return;
         for (int S = 0; S < 2; S++)
             for (int timing = 0; timing < 2; timing++) {
                 cudaGraph_t& g = timing ? tgraph_[S] : graph_[S];
                 cudaGraphExec_t& ex = timing ? texec_[S] : exec_[S];
                 check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-                capture_step(S, timing);
+                enqueue_step(S, timing, false);
                 check(cudaStreamEndCapture(stream_, &g));
                 check(cudaGraphInstantiate(&ex, g, 0));
             }
@@ -692,6 +713,7 @@ private:
     DeviceArena arena_;
     cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
     int par_ = 0;
+    bool eager_ = false;
     std::vector<int> pending_;
     long long steps_before_ = 0;
     // fields: three buffer sets of velocity, impulse and potential (state, stage outputs)
