@@ -97,6 +97,14 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 CavitySolver* cavity_default(void);
 /* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */
 int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
+/* One pass of the fast-diagonalisation pressure solve on caller-provided device arrays (the operation of
+ * backend.cu:801-814 without the rms scaling): phi += S_x S_y S_z (inv_lambda .* (S_z^T S_y^T S_x^T r)), each
+ * S applied along its axis.  s[a] / st[a]: the row-major n_a x n_a eigenbasis of axis a (eigenvector j in
+ * column j) and its transpose; inv_lambda, r, phi: nx*ny*nz doubles, [z][y][x] with x fastest.  All are
+ * device pointers.  Runs on `stream` (a cudaStream_t, NULL for the default stream), allocates its two
+ * nx*ny*nz intermediates on that stream, and returns when phi is updated. */
+int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                    const double* inv_lambda, const double* r, double* phi, void* stream);
 /* Pressure passes run by this cavity since it was created (all stages, steps and projections). */
 long long cavity_pressure_passes(const CavitySolver* s);
 const char* cavity_last_error(void);

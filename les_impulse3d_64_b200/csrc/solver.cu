@@ -21,6 +21,7 @@
 
 #include "cavity_solver.h"
 #include "kernels.cuh"
+#include "fdm.cuh"
 #include "outputs.cuh"
 #include "setup.h"
 
@@ -446,6 +447,9 @@ private:
                         zero ? 0.0 : 1.0 / (e[2].lambda[z] + e[1].lambda[y] + e[0].lambda[x]);
                 }
         check(cudaMemcpy(inv_lambda_, inv.data(), sizeof(double) * n_cell_, cudaMemcpyHostToDevice));
+        fdm_.nx = nx_; fdm_.ny = ny_; fdm_.nz = nz_;
+        for (int a = 0; a < 3; a++) { fdm_.s[a] = S_[a]; fdm_.st[a] = ST_[a]; }
+        fdm_.inv_lambda = inv_lambda_;
         const std::vector<int> cells = probe_cells(c_, ax_);
         if (!cells.empty()) check(cudaMemcpy(probe_cells_, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
         push_control();
@@ -554,34 +558,9 @@ private:
         a.use_handle = use_h;
         residual_kernel<<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
     }
-    template <int BM, int BN, int BK, int TM, int TN>
-    void gemm(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda, long long sA,
-              const double* B, int ldb, long long sB, double* C, int ldc, long long sC, int batch, int epi, double* phi,
-              cudaGraphConditionalHandle h = 0, bool clear = false) {
-        GemmArgs<double> g;
-        g.handle = h;
-        g.clear_condition = clear;
-        g.M = M; g.N = N; g.K = K; g.lda = lda; g.ldb = ldb; g.ldc = ldc;
-        g.sA = sA; g.sB = sB; g.sC = sC;
-        g.A = A; g.A_alt = A_alt; g.B = B; g.C = C;
-        g.inv_lambda = inv_lambda_;
-        g.phi = phi;
-        g.epilogue = epi;
-        g.c = ctrl_;
-        dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch);
-        gemm_kernel<double, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(g);
-    }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
-        const int plane = nx_ * ny_;
-        const long long pl = plane;
-        gemm<32, 32, 8, 2, 2>(st, ny_ * nz_, nx_, nx_, res_, rhs_, nx_, 0, S_[0], nx_, 0, t1_, nx_, 0, 1, kStore, nullptr,
-                              h, use_h);
-        gemm<32, 32, 8, 2, 2>(st, ny_, nx_, ny_, ST_[1], nullptr, ny_, 0, t1_, nx_, pl, t2_, nx_, pl, nz_, kStore, nullptr);
-        gemm<32, 32, 8, 2, 2>(st, nz_, plane, nz_, ST_[2], nullptr, nz_, 0, t2_, plane, 0, t1_, plane, 0, 1, kScaleInvLambda, nullptr);
-        gemm<32, 32, 8, 2, 2>(st, nz_, plane, nz_, S_[2], nullptr, nz_, 0, t1_, plane, 0, t2_, plane, 0, 1, kStore, nullptr);
-        gemm<32, 32, 8, 2, 2>(st, ny_, nx_, ny_, S_[1], nullptr, ny_, 0, t2_, nx_, pl, t1_, nx_, pl, nz_, kStore, nullptr);
-        gemm<32, 32, 8, 2, 2>(st, ny_ * nz_, nx_, nx_, t1_, nullptr, nx_, 0, ST_[0], nx_, 0, nullptr, nx_, 0, 1, kAccumulate, phi);
+        launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h);
         launch_residual(st, phi, false, true, h, use_h);
     }
     void launch_finish(cudaStream_t st, T* const m[3], T* const u_out[3], double* phi, bool step_mode, int stage, bool last) {
@@ -723,6 +702,7 @@ private:
     T* M0_[3];
     double *phi0_, *base_, *rhs_, *res_, *hist_[4], *t1_, *t2_, *inv_lambda_;
     double *S_[3], *ST_[3];
+    FdmOperands fdm_;
     double* partial_;
     long long partial_blocks_;
     Control* ctrl_;
@@ -751,6 +731,36 @@ static long long estimate_bytes(const CavityConfig& c, int precision) {
     const long long maxface = std::max((nx + 1) * ny * nz, nx * ny * (nz + 1));
     return 7 * faces * fb + 16 * cells * 8 + 2 * 8 * maxface + 4 * std::max(maxface, 2 * cells) +
            2 * 8 * (nx * nx + ny * ny + nz * nz) + 64 * (maxface / 256 + 8) + (1 << 20);
+}
+
+// One FDM pass on caller-provided device arrays; the two intermediates are allocated on the stream.
+static void fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                     const double* inv_lambda, const double* r, double* phi, cudaStream_t stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || nx > 1024 || ny > 1024 || nz > 1024) fail("fdm pass: 1 <= nx, ny, nz <= 1024");
+    if (!inv_lambda || !r || !phi) fail("fdm pass: null pointer");
+    FdmOperands op;
+    op.nx = nx; op.ny = ny; op.nz = nz;
+    for (int a = 0; a < 3; a++) {
+        if (!s[a] || !st[a]) fail("fdm pass: null eigenbasis");
+        op.s[a] = s[a];
+        op.st[a] = st[a];
+    }
+    op.inv_lambda = inv_lambda;
+    const size_t n = (size_t)nx * ny * nz;
+    double *t1 = nullptr, *t2 = nullptr;
+    Control* c = nullptr;
+    check(cudaMallocAsync((void**)&t1, sizeof(double) * n, stream));
+    check(cudaMallocAsync((void**)&t2, sizeof(double) * n, stream));
+    check(cudaMallocAsync((void**)&c, sizeof(Control), stream));
+    const Control hc = standalone_fdm_control();
+    check(cudaMemcpyAsync(c, &hc, sizeof hc, cudaMemcpyHostToDevice, stream));
+    launch_fdm_pass(stream, op, r, nullptr, phi, t1, t2, c, 0, false);
+    const cudaError_t launched = cudaGetLastError();
+    check(cudaFreeAsync(t1, stream));
+    check(cudaFreeAsync(t2, stream));
+    check(cudaFreeAsync(c, stream));
+    check(launched);
+    check(cudaStreamSynchronize(stream));
 }
 
 }  // namespace cavity
@@ -853,6 +863,10 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 }
 CavitySolver* cavity_default(void) { return g_default; }
 int cavity_kernels_per_step(const CavitySolver* s, int passes) { return s && s->s ? s->s->kernels_per_step(passes) : -1; }
+int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                    const double* inv_lambda, const double* r, double* phi, void* stream) {
+    return safely([&] { cavity::fdm_pass(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
+}
 long long cavity_pressure_passes(const CavitySolver* s) { return s && s->s ? s->s->pressure_passes() : -1; }
 const char* cavity_last_error(void) { return g_last_error.c_str(); }
 }
