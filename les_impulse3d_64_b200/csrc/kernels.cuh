@@ -672,13 +672,15 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN)) gemm_kernel(GemmArgs<D>
 // u = m - grad(phi) with phi's mean removed (backend.cu:846, 361-371); the potential increment history
 // (backend.cu:929-939); in the last stage the CFL rate of the new velocity for the next step's dt
 // (backend.cu:465-472) and the clock update (backend.cu:945-954).  One thread per cell; the thread of the
-// last cell along an axis also writes the wall face beyond it.
+// last cell along an axis also writes the wall face beyond it.  The solution is read from one buffer and the
+// mean-removed potential written to another, since every thread also reads its neighbours' values.
 template <class T> struct FinishArgs {
     Params p;
     Geo<T> g;
     const T* m[3];
     T* u_out[3];
-    double* phi;               // in: solution, out: mean removed
+    const double* phi;         // the pressure solution (read only: neighbours read it too)
+    double* phi_out;           // the solution with its mean removed
     const double* base;        // step only: for the history increment
     double* hist[4];
     int step_mode;             // 1: stage of a step, 0: plain projection (initialize / kick)
@@ -687,14 +689,6 @@ template <class T> struct FinishArgs {
     Control* c;
     double* partial;
 };
-
-template <class T>
-__device__ __forceinline__ T grad_face(const FinishArgs<T>& a, int comp, int i_lo_cell, int i_cell, int idx_pos,
-                                       double mean) {
-    // d = (phi[c] - phi[c-1]) / spacing, with the mean removed from both values first
-    const double d = ((a.phi[i_cell] - mean) - (a.phi[i_lo_cell] - mean)) * a.g.dinv_sp[comp][idx_pos];
-    return (T)d;
-}
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
@@ -740,7 +734,7 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
                         fmax(fabs(wf[0]), fabs(wf[1])) / tab(a.g, Z, kW, z);
             acc.v[0] = (double)r;
         }
-        a.phi[i] = ph;
+        a.phi_out[i] = ph;
         if (hb >= 0) a.hist[hb][i] = 1.0 * ph + -1.0 * a.base[i];
     }
     // gridwide: CFL max (NaN wins) and the scalar bookkeeping in the last block

@@ -377,6 +377,7 @@ private:
         }
         for (int k = 0; k < 3; k++) M0_[k] = arena_.alloc<T>(size_[k]);
         phi0_ = arena_.alloc<double>(n_cell_);
+        praw_ = arena_.alloc<double>(n_cell_);
         base_ = arena_.alloc<double>(n_cell_);
         rhs_ = arena_.alloc<double>(n_cell_);
         res_ = arena_.alloc<double>(n_cell_);
@@ -536,7 +537,7 @@ private:
         a.phi0 = phi0_;
         a.phi_cur = PHI_[cur];
         a.base = step_mode ? base_ : nullptr;
-        a.guess = PHI_[out];
+        a.guess = praw_;
         for (int k = 0; k < 4; k++) a.hist[k] = hist_[k];
         a.stage = stage;
         a.c = ctrl_;
@@ -563,12 +564,14 @@ private:
         launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h);
         launch_residual(st, phi, false, true, h, use_h);
     }
-    void launch_finish(cudaStream_t st, T* const m[3], T* const u_out[3], double* phi, bool step_mode, int stage, bool last) {
+    void launch_finish(cudaStream_t st, T* const m[3], T* const u_out[3], double* phi_out, bool step_mode, int stage,
+                       bool last) {
         FinishArgs<T> a;
         a.p = p_;
         a.g = geo_;
         for (int k = 0; k < 3; k++) { a.m[k] = m[k]; a.u_out[k] = u_out[k]; }
-        a.phi = phi;
+        a.phi = praw_;
+        a.phi_out = phi_out;
         a.base = base_;
         for (int k = 0; k < 4; k++) a.hist[k] = hist_[k];
         a.step_mode = step_mode;
@@ -624,7 +627,7 @@ private:
             launch_momentum(stream_, stage, S, in, out);
             if (timing) mark(kev_[2 * stage + 1]);
             launch_divergence(stream_, M_[out], true, stage, S, cur, out);
-            double* phi = PHI_[out];
+            double* phi = praw_;          // the solve works here; finish writes PHI_[out]
             if (eager) {
                 launch_residual(stream_, phi, true, true, 0, false);
                 pull_control();
@@ -636,7 +639,7 @@ private:
                 captured_loop([&](cudaGraphConditionalHandle h) { launch_residual(stream_, phi, true, true, h, true); },
                               phi);
             }
-            launch_finish(stream_, M_[out], U_[out], phi, true, stage, stage == 2);
+            launch_finish(stream_, M_[out], U_[out], PHI_[out], true, stage, stage == 2);
         }
     }
 
@@ -663,11 +666,11 @@ private:
         push_control();
         for (int k = 0; k < 3; k++) zero_walls_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(p_, k, m[k]);
         launch_divergence(stream_, m, false, 0, par_, par_, par_);
-        launch_residual(stream_, phi, true, false, 0, false);
+        launch_residual(stream_, praw_, true, false, 0, false);
         pull_control();
         int guard = 0;
         while (hc_.cond && !hc_.error && guard++ < 1000) {
-            launch_pass(stream_, phi, 0, false);
+            launch_pass(stream_, praw_, 0, false);
             pull_control();
         }
         if (hc_.error) {
@@ -700,7 +703,7 @@ private:
     T* M_[3][3];
     double* PHI_[3];
     T* M0_[3];
-    double *phi0_, *base_, *rhs_, *res_, *hist_[4], *t1_, *t2_, *inv_lambda_;
+    double *phi0_, *praw_, *base_, *rhs_, *res_, *hist_[4], *t1_, *t2_, *inv_lambda_;
     double *S_[3], *ST_[3];
     FdmOperands fdm_;
     double* partial_;

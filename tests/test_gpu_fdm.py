@@ -17,8 +17,8 @@ def device(a):
 def fdm_reference(S, r, inv_lambda, phi):
     """phi + S_x S_y S_z (inv_lambda .* S_z^T S_y^T S_x^T r) on [z][y][x] arrays."""
     t = np.einsum('zyi,ij->zyj', r, S[0])
-    t = np.einsum('ij,zix->zjx', S[1].T, t)
-    t = np.einsum('ij,iyx->jyx', S[2].T, t)
+    t = np.einsum('ij,zix->zjx', S[1], t)
+    t = np.einsum('ij,iyx->jyx', S[2], t)
     t = t * inv_lambda
     t = np.einsum('ij,jyx->iyx', S[2], t)
     t = np.einsum('ij,zjx->zix', S[1], t)
