@@ -105,6 +105,18 @@ int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
  * nx*ny*nz intermediates on that stream, and returns when phi is updated. */
 int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                     const double* inv_lambda, const double* r, double* phi, void* stream);
+/* cavity_fdm_pass without any device allocation (no counterpart in the reference).  For callers that must
+ * not allocate device memory themselves or through this library: a host whose device memory is all owned
+ * by its own pool allocator, or a process running with the device nearly full, where a cudaMalloc would
+ * fail or a cudaFree would stall every stream.  Same arguments and result as cavity_fdm_pass; the caller
+ * still passes every input and output.  The two intermediates live in a file-scope device array of
+ * 2 x 262144 doubles (4 MiB, with a control block) that every GPU loading the library holds until the
+ * process exits, so nx*ny*nz is limited to 262144 cells (64^3); larger grids are rejected with an error.
+ * The first call on each device looks up the array's device address once (set-up); make that first call
+ * before any stream capture.  All calls on a device share the array, which keeps the last call's contents:
+ * each call resets the control flags that must start at zero, and calls that overlap on the GPU race. */
+int cavity_fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                            const double* inv_lambda, const double* r, double* phi, void* stream);
 /* Pressure passes run by this cavity since it was created (all stages, steps and projections). */
 long long cavity_pressure_passes(const CavitySolver* s);
 const char* cavity_last_error(void);

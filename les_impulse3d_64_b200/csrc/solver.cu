@@ -766,6 +766,67 @@ static void fdm_pass(int nx, int ny, int nz, const double* const s[3], const dou
     check(cudaStreamSynchronize(stream));
 }
 
+// ------------------------------------------------------------------------------------------ no-allocation pass
+// The FDM pass for callers that cannot allocate device memory: its two intermediates and its control block
+// live in file-scope device arrays instead of cudaMallocAsync'd buffers.  Every GPU that loads the library
+// holds these 4 MiB until the process exits; all calls on a device share them.
+constexpr long long kNoAllocMaxCells = 262144;                      // 64^3
+static __device__ __align__(256) double g_noalloc_transforms[2 * kNoAllocMaxCells];
+static __device__ __align__(256) Control g_noalloc_control;
+
+struct NoAllocScratch {
+    double* transforms = nullptr;
+    Control* control = nullptr;
+};
+static std::mutex g_noalloc_mutex;
+static NoAllocScratch g_noalloc_scratch[64];                        // per device, filled on first use
+
+// Device addresses of the arrays on the current device (host code cannot use their names as addresses).
+static NoAllocScratch noalloc_scratch() {
+    int dev = 0;
+    check(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail("fdm pass (no allocation): device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocScratch& s = g_noalloc_scratch[dev];
+    if (!s.transforms) {
+        void* t = nullptr;
+        void* c = nullptr;
+        check(cudaGetSymbolAddress(&t, g_noalloc_transforms));
+        check(cudaGetSymbolAddress(&c, g_noalloc_control));
+        s.transforms = (double*)t;
+        s.control = (Control*)c;
+    }
+    return s;
+}
+
+static void fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                             const double* inv_lambda, const double* r, double* phi, cudaStream_t stream) {
+    if (nx < 1 || ny < 1 || nz < 1) fail("fdm pass (no allocation): nx, ny, nz must be >= 1");
+    const long long n = (long long)nx * ny * nz;
+    if (n > kNoAllocMaxCells) {
+        char msg[200];
+        std::snprintf(msg, sizeof msg, "fdm pass (no allocation): %d x %d x %d = %lld cells exceeds the maximum of %lld",
+                      nx, ny, nz, n, kNoAllocMaxCells);
+        fail(msg);
+    }
+    if (!inv_lambda || !r || !phi) fail("fdm pass (no allocation): null pointer");
+    FdmOperands op;
+    op.nx = nx; op.ny = ny; op.nz = nz;
+    for (int a = 0; a < 3; a++) {
+        if (!s[a] || !st[a]) fail("fdm pass (no allocation): null eigenbasis");
+        op.s[a] = s[a];
+        op.st[a] = st[a];
+    }
+    op.inv_lambda = inv_lambda;
+    const NoAllocScratch scratch = noalloc_scratch();
+    // the control block keeps the previous call's contents: reset its flags (error, reset) to zero
+    const Control hc = standalone_fdm_control();
+    check(cudaMemcpyAsync(scratch.control, &hc, sizeof hc, cudaMemcpyHostToDevice, stream));
+    launch_fdm_pass(stream, op, r, nullptr, phi, scratch.transforms, scratch.transforms + n, scratch.control, 0, false);
+    check(cudaGetLastError());
+    check(cudaStreamSynchronize(stream));
+}
+
 }  // namespace cavity
 
 // ================================================================================================ C ABI
@@ -869,6 +930,10 @@ int cavity_kernels_per_step(const CavitySolver* s, int passes) { return s && s->
 int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                     const double* inv_lambda, const double* r, double* phi, void* stream) {
     return safely([&] { cavity::fdm_pass(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
+}
+int cavity_fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                            const double* inv_lambda, const double* r, double* phi, void* stream) {
+    return safely([&] { cavity::fdm_pass_noalloc(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
 }
 long long cavity_pressure_passes(const CavitySolver* s) { return s && s->s ? s->s->pressure_passes() : -1; }
 const char* cavity_last_error(void) { return g_last_error.c_str(); }
