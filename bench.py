@@ -45,22 +45,28 @@ def parse_args():
 
 # ------------------------------------------------------------------------------------------ ranks
 class Ranks:
-    """torch.distributed plumbing for N replicas (barrier and max over ranks); identity at N = 1."""
+    """torch.distributed plumbing for N replicas (barrier and max over ranks); identity at N = 1.
 
-    def __init__(self, gpus):
+    One process per GPU: with torchrun, LOCAL_RANK's GPU becomes this process's device 0 before CUDA starts.
+    `backend` is 'nccl' on GPUs; 'gloo' runs the same plumbing on CPU (tests).
+    """
+
+    def __init__(self, backend='nccl'):
         self.world = int(os.environ.get('WORLD_SIZE', '1'))
         self.rank = int(os.environ.get('RANK', '0'))
         self.local = int(os.environ.get('LOCAL_RANK', '0'))
-        self.pg = None
+        self.backend = backend
         if self.world > 1:
-            # one GPU per rank: make it device 0 of this process before CUDA starts
-            os.environ['CUDA_VISIBLE_DEVICES'] = str(self.local)
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(0)
-            dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120), device_id=torch.device('cuda', 0))
+            kw = {}
+            if backend == 'nccl':
+                os.environ['CUDA_VISIBLE_DEVICES'] = str(self.local)
+                torch.cuda.set_device(0)
+                kw['device_id'] = torch.device('cuda', 0)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
             self.dist, self.torch = dist, torch
 
     def barrier(self):
@@ -70,7 +76,7 @@ class Ranks:
     def max(self, x):
         if self.world == 1:
             return x
-        t = self.torch.tensor([float(x)], device='cuda')
+        t = self.torch.tensor([float(x)], device='cuda' if self.backend == 'nccl' else 'cpu')
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -227,7 +233,7 @@ def run_ours(args, ranks):
     launches = args.steps * cav.kernels_per_step(0) + 7 * passes_in_timed(passes, args, cav)
     cav.close()
     total_ms = ranks.max(float(ms.sum()))
-    value = ranks.world * cells * args.steps / (total_ms / 1e3)
+    value = replica_rate(ranks.world, cells, args.steps, total_ms)
 
     # end to end through the reference-facing ABI with host buffers
     sim = Solver(s, precision=precision)
@@ -275,6 +281,12 @@ def run_ours(args, ranks):
     return line
 
 
+def replica_rate(world, cells, steps, max_ms):
+    """Whole-job cell-updates/s of `world` replicas that each advanced `cells` cells by `steps` steps, timed
+    by the slowest rank."""
+    return world * cells * steps / (max_ms / 1e3)
+
+
 def passes_in_timed(passes, args, cav):
     # passes counted over warm-up + timed steps; scale to the timed steps
     total = args.steps + args.warmup
@@ -306,7 +318,7 @@ def run_reference(args, ranks):
 
 def main():
     args = parse_args()
-    ranks = Ranks(args.gpus)
+    ranks = Ranks()
     try:
         line = run_ours(args, ranks) if args.impl == 'ours' else run_reference(args, ranks)
         if line is not None and ranks.rank == 0:

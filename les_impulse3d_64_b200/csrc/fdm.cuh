@@ -16,7 +16,101 @@ struct FdmOperands {
     const double* inv_lambda;
 };
 
-template <int BM, int BN, int BK, int TM, int TN>
+// C[b] = A[b] (M x K) * B[b] (K x N), row-major, on the FP64 tensor cores: each warp owns a 32 x 32 tile of C as
+// fragments of mma.sync.m8n8k4.f64 (the FP64 MMA of sm_80 and later; Blackwell's tcgen05 has no FP64
+// kind).  Operand panels are staged in shared memory with row pitches of 8 banks mod 32, so the 8 x 4 A
+// fragments and 4 x 8 B fragments load without bank conflicts.  Same operand selection, skip rule,
+// loop guard and epilogues as described at GemmArgs (kernels.cuh).
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* src, int src_bytes) {
+    const unsigned int dst = (unsigned int)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// CTA tile BM x BN from WARPS_M x WARPS_N warps; K consumed in panels of KC with every load of a panel in
+// flight at once (cp.async, zero-filled outside the matrices).
+template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
+__global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_kernel(GemmArgs<double> g) {
+    constexpr int NT = WARPS_M * WARPS_N * 32;
+    constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;     // warp tile
+    constexpr int FM = WTM / 8, FN = WTN / 8;                   // fragments per warp tile
+    constexpr int LDA = KC + 4, LDB = BN + 4;                   // row pitches of 8 banks mod 32
+    __shared__ double As[BM * LDA];
+    __shared__ double Bs[KC * LDB];
+    if (g.clear_condition && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+        cudaGraphSetConditional(g.handle, 0u);
+    const Control* c = g.c;
+    if (c->error) return;
+    const double r2 = c->use_rhs ? c->rhs_norm2 : c->res_norm2;       // a zero residual: no pass (backend.cu:803-804)
+    if (!(r2 > 0)) return;
+    const int b = blockIdx.z;
+    const double* A = (g.A_alt && c->use_rhs ? g.A_alt : g.A) + b * g.sA;
+    const double* B = g.B + b * g.sB;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp / WARPS_N, wn = warp % WARPS_N;
+    const int fr = lane >> 2, fc = lane & 3;          // fragment row / column of this lane
+    double acc[FM][FN][2];
+#pragma unroll
+    for (int i = 0; i < FM; i++)
+#pragma unroll
+        for (int j = 0; j < FN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int k0 = 0; k0 < g.K; k0 += KC) {
+        for (int e = threadIdx.x; e < BM * KC; e += NT) {
+            const int r = e / KC, k = e % KC, gm = m0 + r, gk = k0 + k;
+            const bool ok = gm < g.M && gk < g.K;
+            cp_async8(&As[r * LDA + k], ok ? A + (long long)gm * g.lda + gk : A, ok ? 8 : 0);
+        }
+        for (int e = threadIdx.x; e < KC * BN; e += NT) {
+            const int k = e / BN, col = e % BN, gk = k0 + k, gn = n0 + col;
+            const bool ok = gk < g.K && gn < g.N;
+            cp_async8(&Bs[k * LDB + col], ok ? B + (long long)gk * g.ldb + gn : B, ok ? 8 : 0);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        const int kend = min(KC, g.K - k0);
+        for (int kk = 0; kk < kend; kk += 4) {
+            double af[FM], bf[FN];
+#pragma unroll
+            for (int i = 0; i < FM; i++) af[i] = As[(wm * WTM + i * 8 + fr) * LDA + kk + fc];
+#pragma unroll
+            for (int j = 0; j < FN; j++) bf[j] = Bs[(kk + fc) * LDB + wn * WTN + j * 8 + fr];
+#pragma unroll
+            for (int i = 0; i < FM; i++)
+#pragma unroll
+                for (int j = 0; j < FN; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+        __syncthreads();
+    }
+    const int reset = c->reset_phi;
+#pragma unroll
+    for (int i = 0; i < FM; i++) {
+        const int gm = m0 + wm * WTM + i * 8 + fr;
+        if (gm >= g.M) continue;
+#pragma unroll
+        for (int j = 0; j < FN; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int gn = n0 + wn * WTN + j * 8 + 2 * fc + h;
+                if (gn >= g.N) continue;
+                const long long idx = b * g.sC + (long long)gm * g.ldc + gn;
+                const double v = acc[i][j][h];
+                if (g.epilogue == kStore) g.C[idx] = v;
+                else if (g.epilogue == kScaleInvLambda) g.C[idx] = v * g.inv_lambda[idx];
+                else g.phi[idx] = (reset ? 0.0 : g.phi[idx]) + v;
+            }
+    }
+}
+
+// one batched transform launch; the tile shape keeps at least ~two CTAs per SM on small grids
 inline void launch_transform(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda,
                              long long sA, const double* B, int ldb, long long sB, double* C, int ldc, long long sC,
                              int batch, int epi, const double* inv_lambda, double* phi, const Control* c,
@@ -31,8 +125,14 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
     g.phi = phi;
     g.epilogue = epi;
     g.c = c;
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch);
-    gemm_kernel<double, BM, BN, BK, TM, TN><<<grid, (BM / TM) * (BN / TN), 0, st>>>(g);
+    const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch;
+    if (tiles64 >= 296) {
+        dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
+        dgemm_mma_kernel<64, 64, 2, 2, 32><<<grid, 128, 0, st>>>(g);
+    } else {
+        dim3 grid((N + 31) / 32, (M + 31) / 32, batch);
+        dgemm_mma_kernel<32, 32, 2, 2, 64><<<grid, 128, 0, st>>>(g);
+    }
 }
 
 // phi += FDM(r); r_alt replaces r when the control block says use_rhs.  t1, t2: nx*ny*nz doubles of scratch.
@@ -42,17 +142,17 @@ inline void launch_fdm_pass(cudaStream_t st, const FdmOperands& op, const double
     const int nx = op.nx, ny = op.ny, nz = op.nz, plane = nx * ny;
     const long long pl = plane;
     const double* il = op.inv_lambda;
-    launch_transform<32, 32, 8, 2, 2>(st, ny * nz, nx, nx, r, r_alt, nx, 0, op.s[0], nx, 0, t1, nx, 0, 1, kStore, il,
+    launch_transform(st, ny * nz, nx, nx, r, r_alt, nx, 0, op.s[0], nx, 0, t1, nx, 0, 1, kStore, il,
                                       nullptr, c, h, clear);
-    launch_transform<32, 32, 8, 2, 2>(st, ny, nx, ny, op.st[1], nullptr, ny, 0, t1, nx, pl, t2, nx, pl, nz, kStore, il,
+    launch_transform(st, ny, nx, ny, op.st[1], nullptr, ny, 0, t1, nx, pl, t2, nx, pl, nz, kStore, il,
                                       nullptr, c, 0, false);
-    launch_transform<32, 32, 8, 2, 2>(st, nz, plane, nz, op.st[2], nullptr, nz, 0, t2, plane, 0, t1, plane, 0, 1,
+    launch_transform(st, nz, plane, nz, op.st[2], nullptr, nz, 0, t2, plane, 0, t1, plane, 0, 1,
                                       kScaleInvLambda, il, nullptr, c, 0, false);
-    launch_transform<32, 32, 8, 2, 2>(st, nz, plane, nz, op.s[2], nullptr, nz, 0, t1, plane, 0, t2, plane, 0, 1, kStore,
+    launch_transform(st, nz, plane, nz, op.s[2], nullptr, nz, 0, t1, plane, 0, t2, plane, 0, 1, kStore,
                                       il, nullptr, c, 0, false);
-    launch_transform<32, 32, 8, 2, 2>(st, ny, nx, ny, op.s[1], nullptr, ny, 0, t2, nx, pl, t1, nx, pl, nz, kStore, il,
+    launch_transform(st, ny, nx, ny, op.s[1], nullptr, ny, 0, t2, nx, pl, t1, nx, pl, nz, kStore, il,
                                       nullptr, c, 0, false);
-    launch_transform<32, 32, 8, 2, 2>(st, ny * nz, nx, nx, t1, nullptr, nx, 0, op.st[0], nx, 0, nullptr, nx, 0, 1,
+    launch_transform(st, ny * nz, nx, nx, t1, nullptr, nx, 0, op.st[0], nx, 0, nullptr, nx, 0, 1,
                                       kAccumulate, il, phi, c, 0, false);
 }
 

@@ -33,7 +33,7 @@ enum ErrorCode : int {
     kResidualNaN = 3,      // backend.cu:838
     kNotConverged = 4,     // backend.cu:840-844
 };
-enum Counter : int { kCntDiv = 0, kCntRes0, kCntRes, kCntFinish, kCntCfl, kNumCounters };
+enum Counter : int { kCntDiv = 0, kCntRes, kCntFinish, kCntCfl, kNumCounters };
 
 struct alignas(16) Control {
     // clock, committed by the last stage of a successful step (backend.cu:945-954)
@@ -71,7 +71,7 @@ struct Params {
 
 
 template <class T> struct Geo {
-    const T* tab[3];             // tab[a][k * stride[a] + i]
+    const T* tab[3];             // tab[a][k * stride[a] + i + kTabOffset]
     int stride[3];
     const double* dw[3];         // widths (double, float-rounded values)
     const double* dinv_sp[3];    // 1/spacing in double
@@ -79,7 +79,7 @@ template <class T> struct Geo {
 };
 
 template <class T> __device__ __forceinline__ T tab(const Geo<T>& g, int a, int k, int i) {
-    return g.tab[a][k * g.stride[a] + i];
+    return g.tab[a][k * g.stride[a] + i + kTabOffset];
 }
 
 // flat index of component C at (x, y, z)
@@ -211,9 +211,7 @@ __device__ __forceinline__ StageConst stage_const(int stage, const Control* c) {
 }
 
 // ------------------------------------------------------------------------------------------ momentum sweep
-// One RK3 stage of the impulse for every face: inviscid term I = Lamb vector - grad(u.m) (backend.cu:102-274)
-// fused with the viscous flux-form Laplacian, wall/lid fluxes and the RK combination (backend.cu:279-330).
-// Stage 0 also performs the gauge reset m0 = r m + (1-r) u (backend.cu:880-881) on the fly and stores m0.
+// Arguments of the momentum sweep (sweep.cuh): one RK3 stage of the impulse on every face.
 template <class T> struct MomentumArgs {
     Params p;
     Geo<T> g;
@@ -228,161 +226,33 @@ template <class T> struct MomentumArgs {
     T nu;
 };
 
-template <class T> struct MomentumView {
-    const MomentumArgs<T>& a;
-    bool blend;
-    __device__ __forceinline__ T mval(int C, int i) const {
-        const T mv = a.m[C][i];
-        return blend ? a.r * mv + a.one_minus_r * a.u[C][i] : mv;
-    }
-};
-
-// Lamb term of one edge for faces normal to A with tangential axis B: (d u_B/d x_A - d u_A/d x_B) * u_B
-// interpolated along A, times the stencil weight; zero where the edge or its stencil leaves the box.
-template <int A, int B, int Q, class T>
-__device__ __forceinline__ T lamb_edge(const MomentumArgs<T>& a, int ia, int e, int id) {
-    const Params& p = a.p;
-    const int na = A == X ? p.nx : A == Y ? p.ny : p.nz;
-    const int nb = B == X ? p.nx : B == Y ? p.ny : p.nz;
-    const int al = ia - (Q + 1) / 2, ah = ia + (Q - 1) / 2;
-    const int bl = e - (Q + 1) / 2, bh = e + (Q - 1) / 2;
-    if (e < 0 || e > nb || al < 0 || ah > na - 1) return T(0);
-    const T s = tab(a.g, B, kRamp, e) * tab(a.g, A, kRamp, ia);
-    const T wq = Q == 1 ? (p.o4 ? T(1) + s * T(0.125) : T(1)) : -s * T(0.125);
-    if (wq == T(0)) return T(0);
-    if (bl < 0 || bh > nb - 1) return T(0);
-    const T ub_lo = a.u[B][fidx_ab<B, A, B>(p, al, e, id)];
-    const T ub_hi = a.u[B][fidx_ab<B, A, B>(p, ah, e, id)];
-    const T ua_lo = a.u[A][fidx_ab<A, A, B>(p, ia, bl, id)];
-    const T ua_hi = a.u[A][fidx_ab<A, A, B>(p, ia, bh, id)];
-    const T inv_nda = Q == 1 ? tab(a.g, A, kInvSp, ia) : tab(a.g, A, kInvNd3, ia);
-    const T inv_ndb = Q == 1 ? tab(a.g, B, kInvSp, e) : tab(a.g, B, kInvNd3, e);
-    const T o = (ub_hi - ub_lo) * inv_nda - (ua_hi - ua_lo) * inv_ndb;
-    const T ev = Q == 1 ? tab(a.g, A, kEv1Lo, ia) * ub_lo + tab(a.g, A, kEv1Hi, ia) * ub_hi
-                        : tab(a.g, A, kEv3Lo, ia) * ub_lo + tab(a.g, A, kEv3Hi, ia) * ub_hi;
-    return wq * o * ev;
-}
-
-// K = u.m at the centre of cell (x, y, z) (backend.cu:218-222)
-template <class T>
-__device__ __forceinline__ T k_cell(const MomentumView<T>& v, int x, int y, int z) {
-    const Params& p = v.a.p;
-    const int a0 = fidx<X>(p, x, y, z), b0 = fidx<Y>(p, x, y, z), c0 = fidx<Z>(p, x, y, z);
-    const int b1 = b0 + p.nx, c1 = c0 + p.nx * p.ny;
-    const T* const* u = v.a.u;
-    return T(0.5) * ((u[X][a0] * v.mval(X, a0) + u[X][a0 + 1] * v.mval(X, a0 + 1)) +
-                     (u[Y][b0] * v.mval(Y, b0) + u[Y][b1] * v.mval(Y, b1)) +
-                     (u[Z][c0] * v.mval(Z, c0) + u[Z][c1] * v.mval(Z, c1)));
-}
-
-template <int A, int Q, class T>
-__device__ __forceinline__ T lamb_q(const MomentumArgs<T>& a, const int q[3]) {
-    // tangential axes in the reference's order (backend.cu:235-236, 252-253, 269-270)
-    constexpr int B1 = A == X ? Y : A == Y ? X : Y;
-    constexpr int B2 = A == X ? Z : A == Y ? Z : X;
-    constexpr int D1 = 3 - A - B1, D2 = 3 - A - B2;
-    constexpr int up = (Q + 1) / 2, down = (Q - 1) / 2;
-    const T c = Q == 1 ? T(0.5) : tab(a.g, A, kC3, q[A]);
-    T L = c * (lamb_edge<A, B1, Q>(a, q[A], q[B1] + up, q[D1]) + lamb_edge<A, B1, Q>(a, q[A], q[B1] - down, q[D1]));
-    L = L + c * (lamb_edge<A, B2, Q>(a, q[A], q[B2] + up, q[D2]) + lamb_edge<A, B2, Q>(a, q[A], q[B2] - down, q[D2]));
-    return L;
-}
-
-template <int A, class T>
-__device__ void momentum_face(const MomentumArgs<T>& a, const StageConst& sc, T dt, T lidv, int x, int y, int z) {
-    const Params& p = a.p;
-    const int q[3] = {x, y, z};
-    const int n[3] = {p.nx, p.ny, p.nz};
-    const int i = fidx<A>(p, x, y, z);
-    const MomentumView<T> v{a, a.stage == 0};
-    if (a.stage == 0) a.m0_out[A][i] = v.mval(A, i);
-    if (q[A] == 0 || q[A] == n[A]) { a.out[A][i] = T(0); return; }
-    // inviscid term
-    T L = T(0);
-    L = L + lamb_q<A, 1>(a, q);
-    if (p.o4) {
-        // the two halves of the q=3 sum are added separately, in the reference's order
-        constexpr int B1 = A == X ? Y : A == Y ? X : Y;
-        constexpr int B2 = A == X ? Z : A == Y ? Z : X;
-        constexpr int D1 = 3 - A - B1, D2 = 3 - A - B2;
-        const T c = tab(a.g, A, kC3, q[A]);
-        L = L + c * (lamb_edge<A, B1, 3>(a, q[A], q[B1] + 2, q[D1]) + lamb_edge<A, B1, 3>(a, q[A], q[B1] - 1, q[D1]));
-        L = L + c * (lamb_edge<A, B2, 3>(a, q[A], q[B2] + 2, q[D2]) + lamb_edge<A, B2, 3>(a, q[A], q[B2] - 1, q[D2]));
-    }
-    {
-        int lo[3] = {x, y, z};
-        lo[A]--;
-        L = L - (k_cell(v, x, y, z) - k_cell(v, lo[0], lo[1], lo[2])) * tab(a.g, A, kInvSp, q[A]);
-    }
-    // viscous flux-form Laplacian with wall and lid fluxes (backend.cu:289-325)
-    const T cc = v.mval(A, i);
-    const T wall = a.u[A][i];
-    const int ex = p.nx + (A == X), exy = ex * (p.ny + (A == Y));
-    const int stride[3] = {1, ex, exy};
-    T lap = T(0);
-#pragma unroll
-    for (int t = 0; t < 3; t++) {
-        const int s = stride[t];
-        if (t == A) {
-            lap = lap + ((v.mval(A, i + s) - cc) * tab(a.g, t, kInvW, q[t]) -
-                         (cc - v.mval(A, i - s)) * tab(a.g, t, kInvW, q[t] - 1)) * tab(a.g, t, kInvSp, q[t]);
-            continue;
-        }
-        T hi = q[t] < n[t] - 1 ? (v.mval(A, i + s) - cc) * tab(a.g, t, kInvSp, q[t] + 1) : T(0);
-        T lo = q[t] > 0 ? (cc - v.mval(A, i - s)) * tab(a.g, t, kInvSp, q[t]) : T(0);
-        if (q[t] == 0) lo = wall * tab(a.g, t, kInvSp, 0);
-        if (q[t] == n[t] - 1) {
-            if (t == Y) {
-                const T U = A == X ? lidv * a.g.lid_u[x + (p.nx + 1) * z] : T(0);
-                hi = (U - wall) * tab(a.g, Y, kInvSp, n[Y]);
-            } else {
-                hi = -wall * tab(a.g, t, kInvSp, n[t]);
-            }
-        }
-        lap = lap + (hi - lo) * tab(a.g, t, kInvW, q[t]);
-    }
-    T val = cc + dt * (a.nu * lap + L);
-    if (a.stage > 0) val = T(sc.a0) * a.m0[A][i] + T(sc.b) * val;
-    a.out[A][i] = val;
-}
-
-// grid: (ceil(max faces / kThreads), 3); blockIdx.y = component
-template <class T>
-__global__ void __launch_bounds__(kThreads) momentum_kernel(MomentumArgs<T> a) {
-    if (a.c->error) return;
-    const Params& p = a.p;
-    const int comp = blockIdx.y;
-    const int ex = p.nx + (comp == 0), ey = p.ny + (comp == 1), ez = p.nz + (comp == 2);
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= ex * ey * ez) return;
-    const int x = i % ex, y = (i / ex) % ey, z = i / (ex * ey);
-    const StageConst sc = stage_const(a.stage, a.c);
-    const T dt = (T)a.c->dt;
-    const T lidv = (T)lid_speed(p, sc.tau);
-    if (comp == 0) momentum_face<X>(a, sc, dt, lidv, x, y, z);
-    else if (comp == 1) momentum_face<Y>(a, sc, dt, lidv, x, y, z);
-    else momentum_face<Z>(a, sc, dt, lidv, x, y, z);
-}
-
-// ------------------------------------------------------------------------------------------ divergence
-// rhs = volume * div(m) in FP64 (backend.cu:334-342); in a step also the potential carried by the RK
-// combination (base, backend.cu:922-923), the warm-start guess (backend.cu:924-925, 857-873) and, in stage 0,
-// the gauge-reset potential phi0 = r phi (backend.cu:882).
-template <class T> struct DivergenceArgs {
+// ------------------------------------------------------------------------------------------ start of a projection
+// rhs = volume * div(m) in FP64 (backend.cu:334-342) and the residual r = rhs - L guess of the starting potential
+// (backend.cu:825-829).  In a step the starting potential is the warm-start guess: the potential carried by
+// the RK combination (base, backend.cu:922-923) plus the extrapolated increments (backend.cu:924-925,
+// 857-873), evaluated here at each cell and its six neighbours; stage 0 also stores phi0 = r phi
+// (backend.cu:882).  A plain projection (initialize, kick) starts from zero.  The last block takes the
+// reference's start-of-solve decisions (backend.cu:818-831): NaN right-hand side (error), zero right-hand side
+// (phi = 0, no pass), a guess no better than zero (dropped: start from phi = 0 with r = rhs), and whether the
+// refinement loop runs.  Grid-stride over cells.
+template <class T> struct StartArgs {
     Params p;
     Geo<T> g;
     const T* m[3];
     double* rhs;
-    // step only (null in a plain projection)
+    double* res;
+    double* guess;              // the starting potential (the buffer the solve refines)
+    // step only (base == nullptr: a plain projection)
     const double* phi_state;    // stage 0: state potential
     double* phi0;               // stage 0 writes, stages 1, 2 read
     const double* phi_cur;      // stages 1, 2: potential of the previous stage
     double* base;
-    double* guess;              // the new potential buffer, initialised with the guess
     const double* hist[4];
     int stage;
     Control* c;
     double* partial;
+    cudaGraphConditionalHandle handle;
+    int use_handle;
 };
 
 __device__ __forceinline__ void guess_coefficients(const Params& p, const Control* c, double tau, double scale,
@@ -418,102 +288,145 @@ __device__ __forceinline__ void guess_coefficients(const Params& p, const Contro
     }
 }
 
+__device__ __forceinline__ void set_loop(Control* c, cudaGraphConditionalHandle h, int use_handle, int cond) {
+    c->cond = cond;
+    if (use_handle) cudaGraphSetConditional(h, cond ? 1u : 0u);
+}
+
+// decision after a residual: more passes, convergence, or the non-convergence error (backend.cu:832-845)
+__device__ __forceinline__ void decide_loop(const Params& p, Control* c, cudaGraphConditionalHandle h, int use_handle) {
+    const int more = c->rel > p.fdm_rtol && c->passes < p.fdm_max_passes;
+    if (!more && c->rel > p.fdm_rtol) {
+        c->error = kNotConverged;
+        c->error_value = c->rel;
+        c->error_passes = c->passes;
+    }
+    if (!more) c->phi_rel = c->rel;
+    set_loop(c, h, use_handle, more);
+}
+
 template <class T>
-__global__ void __launch_bounds__(kThreads) divergence_kernel(DivergenceArgs<T> a) {
+__global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T> a) {
     Control* c = a.c;
-    if (c->error) return;
     const Params& p = a.p;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    Vec<1> acc;
-    acc.v[0] = 0.0;
-    if (i < p.n_cell) {
-        const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
-        const double dx = a.g.dw[X][x], dy = a.g.dw[Y][y], dz = a.g.dw[Z][z];
-        const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
-        const double r = ((double)a.m[X][iu + 1] - (double)a.m[X][iu]) * (dy * dz) +
-                         ((double)a.m[Y][iv + p.nx] - (double)a.m[Y][iv]) * (dx * dz) +
-                         ((double)a.m[Z][iw + p.nx * p.ny] - (double)a.m[Z][iw]) * (dx * dy);
-        a.rhs[i] = r;
-        acc.v[0] = r * r;
-        if (a.base) {
-            const StageConst sc = stage_const(a.stage, c);
-            double base;
-            if (a.stage == 0) {
-                const double phi0 = p.reinit_r * a.phi_state[i];
-                a.phi0[i] = phi0;
-                base = sc.b * phi0;
-            } else {
-                base = sc.a0 * a.phi0[i] + sc.b * a.phi_cur[i];
-            }
-            a.base[i] = base;
-            int b1, b2;
-            double c1, c2;
-            guess_coefficients(p, c, sc.tau, sc.b * c->dt, b1, c1, b2, c2);
-            double g = base;
-            if (b1 >= 0) {
-                const double ex = b2 >= 0 ? c1 * a.hist[b1][i] + c2 * a.hist[b2][i] : c1 * a.hist[b1][i];
-                g = ex + base;
+    const int err = c->error;
+    const bool have_guess = a.base != nullptr;
+    const StageConst sc = stage_const(a.stage, c);
+    int b1 = -1, b2 = -1;
+    double c1 = 0, c2 = 0;
+    if (have_guess) guess_coefficients(p, c, sc.tau, sc.b * c->dt, b1, c1, b2, c2);
+    // base and guess at cell j
+    auto base_at = [&](int j) {
+        return a.stage == 0 ? sc.b * (p.reinit_r * a.phi_state[j]) : sc.a0 * a.phi0[j] + sc.b * a.phi_cur[j];
+    };
+    auto guess_from = [&](double base, int j) {
+        if (b1 < 0) return base;
+        const double ex = b2 >= 0 ? c1 * a.hist[b1][j] + c2 * a.hist[b2][j] : c1 * a.hist[b1][j];
+        return ex + base;
+    };
+    auto guess_at = [&](int j) { return guess_from(base_at(j), j); };
+    Vec<3> acc;
+    acc.v[0] = acc.v[1] = acc.v[2] = 0.0;
+    const int sy = p.nx, sz = p.nx * p.ny;
+    if (!err) {
+        for (int i = blockIdx.x * kThreads + threadIdx.x; i < p.n_cell; i += gridDim.x * kThreads) {
+            const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
+            const double dx = a.g.dw[X][x], dy = a.g.dw[Y][y], dz = a.g.dw[Z][z];
+            const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
+            const double rhs = ((double)a.m[X][iu + 1] - (double)a.m[X][iu]) * (dy * dz) +
+                               ((double)a.m[Y][iv + p.nx] - (double)a.m[Y][iv]) * (dx * dz) +
+                               ((double)a.m[Z][iw + p.nx * p.ny] - (double)a.m[Z][iw]) * (dx * dy);
+            a.rhs[i] = rhs;
+            acc.v[0] += rhs * rhs;
+            double r = rhs, g = 0.0;
+            if (have_guess) {
+                const double base = base_at(i);
+                if (a.stage == 0) a.phi0[i] = p.reinit_r * a.phi_state[i];
+                a.base[i] = base;
+                g = guess_from(base, i);
+                double s = 0.0;           // L g, backend.cu:352-357
+                if (x + 1 < p.nx) s += (dy * dz) * (guess_at(i + 1) - g) * a.g.dinv_sp[X][x + 1];
+                if (x > 0) s -= (dy * dz) * (g - guess_at(i - 1)) * a.g.dinv_sp[X][x];
+                if (y + 1 < p.ny) s += (dx * dz) * (guess_at(i + sy) - g) * a.g.dinv_sp[Y][y + 1];
+                if (y > 0) s -= (dx * dz) * (g - guess_at(i - sy)) * a.g.dinv_sp[Y][y];
+                if (z + 1 < p.nz) s += (dx * dy) * (guess_at(i + sz) - g) * a.g.dinv_sp[Z][z + 1];
+                if (z > 0) s -= (dx * dy) * (g - guess_at(i - sz)) * a.g.dinv_sp[Z][z];
+                r = rhs - s;
             }
             a.guess[i] = g;
+            a.res[i] = r;
+            acc.v[1] += r * r;
+            acc.v[2] += g;
         }
     }
-    const Vec<1> blk = block_reduce<1, false>(acc);
+    const Vec<3> blk = block_reduce<3, false>(acc);
     if (publish_partials(blk, a.partial, &c->counter[kCntDiv])) {
-        const Vec<1> tot = final_reduce<1, false>(a.partial);
+        const Vec<3> tot = final_reduce<3, false>(a.partial);
         if (threadIdx.x == 0) {
+            c->counter[kCntDiv] = 0;
+            c->passes = 0;
+            c->phi_passes = 0;
+            c->reset_phi = 0;
+            c->zero_rhs = 0;
+            if (err) { set_loop(c, a.handle, a.use_handle, 0); return; }
             c->rhs_norm2 = tot.v[0];
             c->rhs_norm = sqrt(tot.v[0]);
-            c->zero_rhs = 0;
-            c->phi_passes = 0;
-            c->passes = 0;
-            if (!isfinite(c->rhs_norm)) { c->error = kRhsNaN; c->cond = 0; }
-            else if (c->rhs_norm == 0.0) c->zero_rhs = 1;
-            c->counter[kCntDiv] = 0;
+            if (!isfinite(c->rhs_norm)) { c->error = kRhsNaN; set_loop(c, a.handle, a.use_handle, 0); return; }
+            if (c->rhs_norm == 0.0) {                         // backend.cu:821: phi = 0
+                c->zero_rhs = 1;
+                c->reset_phi = 1;
+                c->phi_rel = 0.0;
+                c->phi_sum = 0.0;
+                c->rel = 0.0;
+                set_loop(c, a.handle, a.use_handle, 0);
+                return;
+            }
+            double rel = 1.0;
+            c->use_rhs = 1;
+            c->phi_sum = 0.0;
+            if (have_guess) {
+                rel = sqrt(tot.v[1]) / c->rhs_norm;
+                c->res_norm2 = tot.v[1];
+                c->use_rhs = 0;
+                c->phi_sum = tot.v[2];
+                if (rel >= 1.0) { rel = 1.0; c->use_rhs = 1; c->reset_phi = 1; c->phi_sum = 0.0; }
+            }
+            c->rel = rel;
+            decide_loop(p, c, a.handle, a.use_handle);
         }
     }
 }
 
 // ------------------------------------------------------------------------------------------ residual
-// r = rhs - L phi with L the 7-point area-weighted Neumann Laplacian (backend.cu:345-359), sum r^2 and
-// sum phi.  `first`: the residual of the warm-start guess (or no guess), which decides the start of the
-// refinement loop (backend.cu:822-831); otherwise the residual after a pass (backend.cu:835-839).
+// r = rhs - L phi with L the 7-point area-weighted Neumann Laplacian (backend.cu:345-359) after a pass, sum r^2
+// and sum phi; the last block counts the pass and decides on the next (backend.cu:835-839).  Grid-stride.
 struct ResidualArgs {
     Params p;
     const double* dw[3];
     const double* dinv_sp[3];
-    double* phi;
+    const double* phi;
     const double* rhs;
     double* res;
-    int first, have_guess;
     Control* c;
     double* partial;
     cudaGraphConditionalHandle handle;
     int use_handle;
 };
 
-__device__ __forceinline__ void set_loop(const ResidualArgs& a, Control* c, int cond) {
-    c->cond = cond;
-    if (a.use_handle) cudaGraphSetConditional(a.handle, cond ? 1u : 0u);
-}
-
 __global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) {
     Control* c = a.c;
     const Params& p = a.p;
     const int err = c->error;
-    const int zero = c->zero_rhs;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
     Vec<2> acc;
     acc.v[0] = 0.0;
     acc.v[1] = 0.0;
-    if (!err && i < p.n_cell) {
-        if (a.first && (zero || !a.have_guess)) {
-            a.phi[i] = 0.0;                    // no guess, or nothing to solve: phi = 0
-        } else {
+    const int sy = p.nx, sz = p.nx * p.ny;
+    if (!err) {
+        for (int i = blockIdx.x * kThreads + threadIdx.x; i < p.n_cell; i += gridDim.x * kThreads) {
             const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
             const double dx = a.dw[X][x], dy = a.dw[Y][y], dz = a.dw[Z][z];
             const double* f = a.phi;
             const double cc = f[i];
-            const int sy = p.nx, sz = p.nx * p.ny;
             double s = 0.0;
             if (x + 1 < p.nx) s += (dy * dz) * (f[i + 1] - cc) * a.dinv_sp[X][x + 1];
             if (x > 0) s -= (dy * dz) * (cc - f[i - 1]) * a.dinv_sp[X][x];
@@ -523,67 +436,35 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) {
             if (z > 0) s -= (dx * dy) * (cc - f[i - sz]) * a.dinv_sp[Z][z];
             const double r = a.rhs[i] - s;
             a.res[i] = r;
-            acc.v[0] = r * r;
-            acc.v[1] = cc;
+            acc.v[0] += r * r;
+            acc.v[1] += cc;
         }
     }
     const Vec<2> blk = block_reduce<2, false>(acc);
-    unsigned int* counter = &c->counter[a.first ? kCntRes0 : kCntRes];
-    if (publish_partials(blk, a.partial, counter)) {
+    if (publish_partials(blk, a.partial, &c->counter[kCntRes])) {
         const Vec<2> tot = final_reduce<2, false>(a.partial);
         if (threadIdx.x == 0) {
-            *counter = 0;
-            if (err) { set_loop(a, c, 0); return; }
-            if (a.first) {
-                c->passes = 0;
-                c->phi_passes = 0;
-                c->reset_phi = 0;
-                if (zero) {                                           // backend.cu:821
-                    c->phi_rel = 0.0;
-                    c->phi_sum = 0.0;
-                    c->rel = 0.0;
-                    set_loop(a, c, 0);
-                    return;
-                }
-                double rel = 1.0;
-                c->use_rhs = 1;
-                c->phi_sum = 0.0;
-                if (a.have_guess) {
-                    rel = sqrt(tot.v[0]) / c->rhs_norm;
-                    c->res_norm2 = tot.v[0];
-                    c->use_rhs = 0;
-                    c->phi_sum = tot.v[1];
-                    if (rel >= 1.0) { rel = 1.0; c->use_rhs = 1; c->reset_phi = 1; c->phi_sum = 0.0; }
-                }
-                c->rel = rel;
-            } else {
-                c->passes += 1;
-                c->phi_passes = c->passes;
-                c->pass_count += 1;
-                c->use_rhs = 0;
-                c->reset_phi = 0;
-                c->res_norm2 = tot.v[0];
-                c->phi_sum = tot.v[1];
-                c->rel = sqrt(tot.v[0]) / c->rhs_norm;
-                if (!isfinite(c->rel)) { c->error = kResidualNaN; set_loop(a, c, 0); return; }
-            }
-            const int more = c->rel > p.fdm_rtol && c->passes < p.fdm_max_passes;
-            if (!more && c->rel > p.fdm_rtol) {
-                c->error = kNotConverged;
-                c->error_value = c->rel;
-                c->error_passes = c->passes;
-            }
-            if (!more) c->phi_rel = c->rel;
-            set_loop(a, c, more);
+            c->counter[kCntRes] = 0;
+            if (err) { set_loop(c, a.handle, a.use_handle, 0); return; }
+            c->passes += 1;
+            c->phi_passes = c->passes;
+            c->pass_count += 1;
+            c->use_rhs = 0;
+            c->reset_phi = 0;
+            c->res_norm2 = tot.v[0];
+            c->phi_sum = tot.v[1];
+            c->rel = sqrt(tot.v[0]) / c->rhs_norm;
+            if (!isfinite(c->rel)) { c->error = kResidualNaN; set_loop(c, a.handle, a.use_handle, 0); return; }
+            decide_loop(p, c, a.handle, a.use_handle);
         }
     }
 }
 
 // ------------------------------------------------------------------------------------------ FDM transforms
-// C[b] = A[b] (M x K) * B[b] (K x N), row-major, batched by strides: the directional transforms of the
-// fast-diagonalisation pressure solve (backend.cu:792-813).  Register-blocked SIMT tiles; the operand that
-// is a residual is chosen on the device (rhs when the guess was rejected, else the residual), the epilogue
-// either stores, scales by 1/lambda, or accumulates into phi.
+// Arguments of the batched transform C[b] = A[b] (M x K) * B[b] (K x N) of the fast-diagonalisation pressure
+// solve (backend.cu:792-813; kernel in fdm.cuh).  The operand that is a residual is chosen on the device (rhs
+// when the guess was rejected, else the residual); the epilogue stores, scales by 1/lambda, or accumulates
+// into phi.
 enum Epilogue : int { kStore = 0, kScaleInvLambda = 1, kAccumulate = 2 };
 
 template <class D> struct GemmArgs {
@@ -602,71 +483,6 @@ template <class D> struct GemmArgs {
     cudaGraphConditionalHandle handle;
     int clear_condition;
 };
-
-template <class D, int BM, int BN, int BK, int TM, int TN>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN)) gemm_kernel(GemmArgs<D> g) {
-    if (g.clear_condition && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
-        cudaGraphSetConditional(g.handle, 0u);
-    const Control* c = g.c;
-    if (c->error) return;
-    // a pass with a zero residual does nothing (backend.cu:803-804)
-    const double r2 = c->use_rhs ? c->rhs_norm2 : c->res_norm2;
-    if (!(r2 > 0)) return;
-    constexpr int NT = (BM / TM) * (BN / TN);
-    __shared__ D As[BK][BM + 1];
-    __shared__ D Bs[BK][BN];
-    const int b = blockIdx.z;
-    const D* A = (g.A_alt && c->use_rhs ? g.A_alt : g.A) + b * g.sA;
-    const D* B = g.B + b * g.sB;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int tx = threadIdx.x % (BN / TN), ty = threadIdx.x / (BN / TN);
-    D acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; i++)
-#pragma unroll
-        for (int j = 0; j < TN; j++) acc[i][j] = D(0);
-    for (int k0 = 0; k0 < g.K; k0 += BK) {
-        for (int e = threadIdx.x; e < BM * BK; e += NT) {
-            const int r = e / BK, k = e % BK;
-            const int gm = m0 + r, gk = k0 + k;
-            As[k][r] = (gm < g.M && gk < g.K) ? A[(long long)gm * g.lda + gk] : D(0);
-        }
-        for (int e = threadIdx.x; e < BK * BN; e += NT) {
-            const int k = e / BN, col = e % BN;
-            const int gk = k0 + k, gn = n0 + col;
-            Bs[k][col] = (gk < g.K && gn < g.N) ? B[(long long)gk * g.ldb + gn] : D(0);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < BK; k++) {
-            D av[TM], bv[TN];
-#pragma unroll
-            for (int i = 0; i < TM; i++) av[i] = As[k][ty + i * (BM / TM)];
-#pragma unroll
-            for (int j = 0; j < TN; j++) bv[j] = Bs[k][tx + j * (BN / TN)];
-#pragma unroll
-            for (int i = 0; i < TM; i++)
-#pragma unroll
-                for (int j = 0; j < TN; j++) acc[i][j] += av[i] * bv[j];
-        }
-        __syncthreads();
-    }
-    const int reset = c->reset_phi;
-#pragma unroll
-    for (int i = 0; i < TM; i++) {
-        const int gm = m0 + ty + i * (BM / TM);
-        if (gm >= g.M) continue;
-#pragma unroll
-        for (int j = 0; j < TN; j++) {
-            const int gn = n0 + tx + j * (BN / TN);
-            if (gn >= g.N) continue;
-            const long long idx = b * g.sC + (long long)gm * g.ldc + gn;
-            if (g.epilogue == kStore) g.C[idx] = acc[i][j];
-            else if (g.epilogue == kScaleInvLambda) g.C[idx] = acc[i][j] * g.inv_lambda[idx];
-            else g.phi[idx] = (reset ? 0.0 : g.phi[idx]) + (double)acc[i][j];
-        }
-    }
-}
 
 // ------------------------------------------------------------------------------------------ finish a projection
 // u = m - grad(phi) with phi's mean removed (backend.cu:846, 361-371); the potential increment history
@@ -695,7 +511,7 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
     Control* c = a.c;
     const Params& p = a.p;
     const int err = c->error;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
+    const int zero_phi = c->reset_phi;       // the solve ended on phi = 0 (zero right-hand side, or no pass)
     Vec<1> acc;
     acc.v[0] = -INFINITY;
     // history buffer for this stage's increment: the first one no entry uses (backend.cu:930-935)
@@ -707,20 +523,21 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
             if (!used) hb = k;
         }
     }
-    if (!err && i < p.n_cell) {
-        const double mean = c->phi_sum / p.n_cell;
+    const double mean = c->phi_sum / p.n_cell;
+    const int sy = p.nx, sz = p.nx * p.ny;
+    auto pv = [&](int j) { return zero_phi ? 0.0 : a.phi[j] - mean; };
+    for (int i = err ? p.n_cell : blockIdx.x * kThreads + threadIdx.x; i < p.n_cell; i += gridDim.x * kThreads) {
         const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
-        const double ph = a.phi[i] - mean;
+        const double ph = pv(i);
         // faces below this cell (wall faces 0), and above it at the last cell of an axis
         const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
-        const int sy = p.nx, sz = p.nx * p.ny;
         T uf[2], vf[2], wf[2];
-        uf[0] = x == 0 ? T(0) : a.m[X][iu] - (T)((ph - (a.phi[i - 1] - mean)) * a.g.dinv_sp[X][x]);
-        vf[0] = y == 0 ? T(0) : a.m[Y][iv] - (T)((ph - (a.phi[i - sy] - mean)) * a.g.dinv_sp[Y][y]);
-        wf[0] = z == 0 ? T(0) : a.m[Z][iw] - (T)((ph - (a.phi[i - sz] - mean)) * a.g.dinv_sp[Z][z]);
-        uf[1] = x == p.nx - 1 ? T(0) : a.m[X][iu + 1] - (T)(((a.phi[i + 1] - mean) - ph) * a.g.dinv_sp[X][x + 1]);
-        vf[1] = y == p.ny - 1 ? T(0) : a.m[Y][iv + p.nx] - (T)(((a.phi[i + sy] - mean) - ph) * a.g.dinv_sp[Y][y + 1]);
-        wf[1] = z == p.nz - 1 ? T(0) : a.m[Z][iw + sz] - (T)(((a.phi[i + sz] - mean) - ph) * a.g.dinv_sp[Z][z + 1]);
+        uf[0] = x == 0 ? T(0) : a.m[X][iu] - (T)((ph - pv(i - 1)) * a.g.dinv_sp[X][x]);
+        vf[0] = y == 0 ? T(0) : a.m[Y][iv] - (T)((ph - pv(i - sy)) * a.g.dinv_sp[Y][y]);
+        wf[0] = z == 0 ? T(0) : a.m[Z][iw] - (T)((ph - pv(i - sz)) * a.g.dinv_sp[Z][z]);
+        uf[1] = x == p.nx - 1 ? T(0) : a.m[X][iu + 1] - (T)((pv(i + 1) - ph) * a.g.dinv_sp[X][x + 1]);
+        vf[1] = y == p.ny - 1 ? T(0) : a.m[Y][iv + p.nx] - (T)((pv(i + sy) - ph) * a.g.dinv_sp[Y][y + 1]);
+        wf[1] = z == p.nz - 1 ? T(0) : a.m[Z][iw + sz] - (T)((pv(i + sz) - ph) * a.g.dinv_sp[Z][z + 1]);
         a.u_out[X][iu] = uf[0];
         a.u_out[Y][iv] = vf[0];
         a.u_out[Z][iw] = wf[0];
@@ -732,7 +549,7 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
             const T r = fmax(fabs(uf[0]), fabs(uf[1])) / tab(a.g, X, kW, x) +
                         fmax(fabs(vf[0]), fabs(vf[1])) / tab(a.g, Y, kW, y) +
                         fmax(fabs(wf[0]), fabs(wf[1])) / tab(a.g, Z, kW, z);
-            acc.v[0] = (double)r;
+            acc.v[0] = combine<1, true>(acc.v[0], (double)r);
         }
         a.phi_out[i] = ph;
         if (hb >= 0) a.hist[hb][i] = 1.0 * ph + -1.0 * a.base[i];

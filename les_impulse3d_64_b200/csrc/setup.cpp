@@ -204,7 +204,7 @@ template <class T>
 std::vector<T> axis_tables(const AxisGrid& g, double ramp_cells, int stride) {
     const int n = g.n;
     std::vector<T> t((size_t)kNumTabs * stride, T(0));
-    auto at = [&](int k, int i) -> T& { return t[(size_t)k * stride + i]; };
+    auto at = [&](int k, int i) -> T& { return t[(size_t)k * stride + i + kTabOffset]; };
     auto w = [&](int i) { return (T)g.width[i]; };
     auto sp = [&](int i) { return (T)g.spacing[i]; };
     const T K = (T)std::max(ramp_cells, 1.0);
@@ -223,12 +223,17 @@ std::vector<T> axis_tables(const AxisGrid& g, double ramp_cells, int stride) {
             at(kEv3Lo, i) = w(i - 2) / (w(i - 2) + w(i + 1));
             at(kEv3Hi, i) = w(i + 1) / (w(i - 2) + w(i + 1));
         }
-        if (i >= 1 && i <= n - 1) {          // narrow (q = 1): cells i-1 and i
+        const bool narrow = i >= 1 && i <= n - 1;       // cells i-1 and i
+        if (narrow) {
             at(kEv1Lo, i) = w(i - 1) / (T(2) * sp(i));
             at(kEv1Hi, i) = w(i) / (T(2) * sp(i));
         }
         const T d = (T)(i < n - i ? i : n - i) - T(1);     // wall ramp (backend.cu:130-133)
         at(kRamp, i) = std::min(std::max(d / K, T(0)), T(1));
+        at(kOk1, i) = narrow ? T(1) : T(0);
+        at(kOk3, i) = wide ? T(1) : T(0);
+        at(kL1, i) = at(kOk1, i) * at(kRamp, i);
+        at(kL3, i) = at(kOk3, i) * at(kRamp, i);
     }
     return t;
 }

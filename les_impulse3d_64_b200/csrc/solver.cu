@@ -22,6 +22,7 @@
 #include "cavity_solver.h"
 #include "kernels.cuh"
 #include "fdm.cuh"
+#include "sweep.cuh"
 #include "outputs.cuh"
 #include "setup.h"
 
@@ -318,7 +319,7 @@ public:
     }
     long long device_bytes() const override { return arena_.bytes(); }
 
-    int kernels_per_step(int passes) const override { return 1 + 3 * 4 + 3 * passes * 7; }
+    int kernels_per_step(int passes) const override { return 1 + 3 * 3 + 3 * passes * 7; }
     long long pressure_passes() const override { return hc_.pass_count; }
 
     void time_steps(int warmup, int steps, int flush, float* ms, float* kms) override {
@@ -386,6 +387,10 @@ private:
         t2_ = arena_.alloc<double>(n_cell_);
         inv_lambda_ = arena_.alloc<double>(n_cell_);
         partial_blocks_ = (long long)blocks_for(std::max(max_face_, n_cell_)) + 8;
+        int sms = 148, dev = 0;
+        check(cudaGetDevice(&dev));
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        cell_blocks_ = (unsigned int)std::min<long long>(blocks_for(n_cell_), 4LL * sms);
         partial_ = arena_.alloc<double>(8 * partial_blocks_);
         ctrl_ = arena_.alloc<Control>(1);
         slots_ = arena_.alloc<double>(kNumSlots);
@@ -404,7 +409,7 @@ private:
         Geo<T>& g = geo_;
         for (int a = 0; a < 3; a++) {
             const AxisGrid& ag = ax_[a];
-            const int stride = ag.n + 2;
+            const int stride = tab_stride(ag.n);
             const std::vector<T> t = axis_tables<T>(ag, c_.impulse_order4_ramp, stride);
             T* d = arena_.alloc<T>((long long)t.size());
             check(cudaMemcpy(d, t.data(), sizeof(T) * t.size(), cudaMemcpyHostToDevice));
@@ -527,42 +532,45 @@ private:
         dim3 grid(blocks_for(max_face_), 3);
         momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
     }
-    void launch_divergence(cudaStream_t st, T* const m[3], bool step_mode, int stage, int S, int cur, int out) {
-        DivergenceArgs<T> a;
+    // rhs, starting potential and its residual, start-of-solve decisions (backend.cu:816-831)
+    void launch_start(cudaStream_t st, T* const m[3], bool step_mode, int stage, int S, int cur,
+                      cudaGraphConditionalHandle h, bool use_h) {
+        StartArgs<T> a;
         a.p = p_;
         a.g = geo_;
         for (int k = 0; k < 3; k++) a.m[k] = m[k];
         a.rhs = rhs_;
+        a.res = res_;
+        a.guess = praw_;
         a.phi_state = PHI_[S];
         a.phi0 = phi0_;
         a.phi_cur = PHI_[cur];
         a.base = step_mode ? base_ : nullptr;
-        a.guess = praw_;
         for (int k = 0; k < 4; k++) a.hist[k] = hist_[k];
         a.stage = stage;
         a.c = ctrl_;
         a.partial = partial_;
-        divergence_kernel<T><<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
+        a.handle = h;
+        a.use_handle = use_h;
+        projection_start_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
     }
-    void launch_residual(cudaStream_t st, double* phi, bool first, bool have_guess, cudaGraphConditionalHandle h, bool use_h) {
+    void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, bool use_h) {
         ResidualArgs a;
         a.p = p_;
         for (int k = 0; k < 3; k++) { a.dw[k] = geo_.dw[k]; a.dinv_sp[k] = geo_.dinv_sp[k]; }
         a.phi = phi;
         a.rhs = rhs_;
         a.res = res_;
-        a.first = first;
-        a.have_guess = have_guess;
         a.c = ctrl_;
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        residual_kernel<<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
+        residual_kernel<<<cell_blocks_, kThreads, 0, st>>>(a);
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
         launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h);
-        launch_residual(st, phi, false, true, h, use_h);
+        launch_residual(st, phi, h, use_h);
     }
     void launch_finish(cudaStream_t st, T* const m[3], T* const u_out[3], double* phi_out, bool step_mode, int stage,
                        bool last) {
@@ -579,7 +587,7 @@ private:
         a.stage = stage;
         a.c = ctrl_;
         a.partial = partial_;
-        finish_kernel<T><<<blocks_for(n_cell_), kThreads, 0, st>>>(a);
+        finish_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
     }
 
     // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
@@ -626,17 +634,16 @@ private:
             if (timing) mark(kev_[2 * stage]);
             launch_momentum(stream_, stage, S, in, out);
             if (timing) mark(kev_[2 * stage + 1]);
-            launch_divergence(stream_, M_[out], true, stage, S, cur, out);
             double* phi = praw_;          // the solve works here; finish writes PHI_[out]
             if (eager) {
-                launch_residual(stream_, phi, true, true, 0, false);
+                launch_start(stream_, M_[out], true, stage, S, cur, 0, false);
                 pull_control();
                 while (hc_.cond && !hc_.error) {
                     launch_pass(stream_, phi, 0, false);
                     pull_control();
                 }
             } else {
-                captured_loop([&](cudaGraphConditionalHandle h) { launch_residual(stream_, phi, true, true, h, true); },
+                captured_loop([&](cudaGraphConditionalHandle h) { launch_start(stream_, M_[out], true, stage, S, cur, h, true); },
                               phi);
             }
             launch_finish(stream_, M_[out], U_[out], PHI_[out], true, stage, stage == 2);
@@ -665,8 +672,7 @@ private:
         hc_.error = kOk;
         push_control();
         for (int k = 0; k < 3; k++) zero_walls_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(p_, k, m[k]);
-        launch_divergence(stream_, m, false, 0, par_, par_, par_);
-        launch_residual(stream_, praw_, true, false, 0, false);
+        launch_start(stream_, m, false, 0, par_, par_, 0, false);
         pull_control();
         int guard = 0;
         while (hc_.cond && !hc_.error && guard++ < 1000) {
@@ -708,6 +714,7 @@ private:
     FdmOperands fdm_;
     double* partial_;
     long long partial_blocks_;
+    unsigned int cell_blocks_ = 1;     // grid of the grid-stride cell kernels: at most 4 CTAs per SM
     Control* ctrl_;
     double *slots_, *stats_, *line_, *dstage_[2];
     unsigned int* out_counters_;

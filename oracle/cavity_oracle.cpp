@@ -615,10 +615,12 @@ struct Oracle {
     }
 
     // ------------------------------------------------------------ CFL rate (backend.cu:465-472)
+    // fmax as the reference's fmaxf: a NaN on one face of the pair is dropped (a single NaN face does not
+    // make the rate NaN; it surfaces later as a NaN right-hand side)
     Real cfl_rate_cell(const vector<Real>* f, int x, int y, int z) const {
-        return std::max(std::fabs(f[0][at(0, x, y, z)]), std::fabs(f[0][at(0, x + 1, y, z)])) / width(X, x) +
-               std::max(std::fabs(f[1][at(1, x, y, z)]), std::fabs(f[1][at(1, x, y + 1, z)])) / width(Y, y) +
-               std::max(std::fabs(f[2][at(2, x, y, z)]), std::fabs(f[2][at(2, x, y, z + 1)])) / width(Z, z);
+        return std::fmax(std::fabs(f[0][at(0, x, y, z)]), std::fabs(f[0][at(0, x + 1, y, z)])) / width(X, x) +
+               std::fmax(std::fabs(f[1][at(1, x, y, z)]), std::fabs(f[1][at(1, x, y + 1, z)])) / width(Y, y) +
+               std::fmax(std::fabs(f[2][at(2, x, y, z)]), std::fabs(f[2][at(2, x, y, z + 1)])) / width(Z, z);
     }
     double cfl_max(const vector<Real>* f) const {
         return det_max(n_cell, [&](long long i) {
