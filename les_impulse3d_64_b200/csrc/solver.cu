@@ -23,6 +23,7 @@
 #include "kernels.cuh"
 #include "fdm.cuh"
 #include "sweep.cuh"
+#include "sweep_tile.cuh"
 #include "outputs.cuh"
 #include "setup.h"
 
@@ -90,6 +91,10 @@ public:
 
 // ------------------------------------------------------------------------------------------ the solver
 template <class T> class Solver : public SolverBase {
+    // tile of the shared-memory sweep: 32 x TY x TZ cells (about 113 KB of shared memory in FP64, 85 KB in FP32)
+    static constexpr int kTileTY = sizeof(T) == 8 ? 4 : 8;
+    static constexpr int kTileTZ = 4;
+
 public:
     explicit Solver(const CavityConfig& cfg) : c_(cfg) {
         const std::string bad = check_config(c_);
@@ -529,8 +534,14 @@ private:
         a.r = (T)c_.reinit_r;
         a.one_minus_r = (T)(1.0 - c_.reinit_r);
         a.nu = (T)c_.nu;
-        dim3 grid(blocks_for(max_face_), 3);
-        momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
+        if (tile_sweep_) {
+            using G = TileGeom<kTileTY, kTileTZ>;
+            dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
+            sweep_tile_kernel<T, kTileTY, kTileTZ><<<grid, kTileThreads, G::template smem_bytes<T>(), st>>>(a);
+        } else {
+            dim3 grid(blocks_for(max_face_), 3);
+            momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
+        }
     }
     // rhs, starting potential and its residual, start-of-solve decisions (backend.cu:816-831)
     void launch_start(cudaStream_t st, T* const m[3], bool step_mode, int stage, int S, int cur,
@@ -651,6 +662,15 @@ private:
     }
 
     void build_graphs() {
+        {
+            // momentum sweep: the shared-memory tile kernel unless CAVITY_SWEEP=face
+            const char* sw = std::getenv("CAVITY_SWEEP");
+            tile_sweep_ = !(sw && std::string(sw) == "face");
+            using G = TileGeom<kTileTY, kTileTZ>;
+            if (tile_sweep_)
+                check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::template smem_bytes<T>()));
+        }
         for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
         const char* env = std::getenv("CAVITY_GRAPHS");
         eager_ = env && env[0] == '0';
@@ -702,6 +722,7 @@ private:
     cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
     int par_ = 0;
     bool eager_ = false;
+    bool tile_sweep_ = true;
     std::vector<int> pending_;
     long long steps_before_ = 0;
     // fields: three buffer sets of velocity, impulse and potential (state, stage outputs)

@@ -1,0 +1,345 @@
+// sweep_tile.cuh - the momentum sweep on a shared-memory tile (the alternative to momentum_kernel, sweep.cuh).
+//
+// A CTA owns a tile of 32 x TY x TZ cells and computes the three lower faces of every cell.  It stages every
+// input of the tile in shared memory first, all copies in flight at once (cp.async):
+//   - the velocity with the halos the 4th-order Lamb stencil reaches: 3 cells across a component's axis, 1-2
+//     along it;
+//   - the impulse with a 1-cell halo; stage 0 applies the gauge-reset blend m0 = r m + (1-r) u
+//     (backend.cu:880-881) while staging;
+//   - the slices of the per-axis coefficient tables the tile uses.
+// Staged values outside the box are clamped copies; every stencil term that reaches them has weight zero.
+// K = u.m (backend.cu:218-222) is computed once per cell.  Each face then evaluates its eight edge terms
+// (vorticity times interpolated velocity: backend.cu:141-215) from shared memory and adds them in the
+// reference's order: narrow then wide stencil, first then second tangential axis (backend.cu:232-238,
+// 249-255, 266-272).  It then adds -grad K, the viscous flux Laplacian with its wall and lid fluxes, and the RK
+// combination (backend.cu:279-330).  The validity rules of the reference's stencils are folded into the weight
+// tables (kOk1, kL1, kL3), so the edge arithmetic has no branches.
+#pragma once
+#include "sweep.cuh"
+
+namespace cavity {
+
+constexpr int kTileThreads = 256;
+
+template <int TY, int TZ> struct TileGeom {
+    static constexpr int TX = 32;
+    static constexpr int ROWS_PER_THREAD = TY * TZ / 8;
+    // velocity boxes: u on x-faces [x0-1, x0+TX+1] x cells [y0-3, y0+TY+2] x [z0-3, z0+TZ+2];
+    // v on cells [x0-3, x0+TX+2] x y-faces [y0-1, y0+TY+1] x cells [z0-3, z0+TZ+2];
+    // w on cells [x0-3, x0+TX+2] x [y0-3, y0+TY+2] x z-faces [z0-1, z0+TZ+1]
+    static constexpr int UW = TX + 3, UH = TY + 6, UD = TZ + 6;
+    static constexpr int VW = TX + 6, VH = TY + 3, VD = TZ + 6;
+    static constexpr int WW = TX + 6, WH = TY + 6, WD = TZ + 3;
+    // impulse boxes: each component on its faces / cells [lo-1, hi] along every axis
+    static constexpr int MW = TX + 2, MH = TY + 2, MD = TZ + 2;
+    static constexpr int NU = UW * UH * UD, NV = VW * VH * VD, NW = WW * WH * WD, NM = MW * MH * MD;
+    static constexpr int NK = (TX + 1) * (TY + 1) * (TZ + 1);  // cells [x0-1, x0+TX) x [y0-1, y0+TY) x [z0-1, z0+TZ)
+    // table slices: indices [lo-2, lo+T+2] of each axis
+    static constexpr int SX = TX + 5, SY = TY + 5, SZ = TZ + 5;
+    static constexpr int NT = kNumTabs * (SX + SY + SZ);
+    static constexpr int ELEMS = NU + NV + NW + 3 * NM + NK + NT;
+    template <class T> static constexpr size_t smem_bytes() { return sizeof(T) * (size_t)ELEMS; }
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* src) {
+    const unsigned int dst = (unsigned int)__cvta_generic_to_shared(smem_dst);
+    if (BYTES == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+}
+
+// Stage a W x H x D box of a face array with extents (ex, ey, ez) and corner (xs, ys, zs), coordinates clamped
+// into the array.  Flattened over the CTA.  With `blend` the box receives r m + (1-r) u.
+template <class T, int W, int H, int D>
+__device__ __forceinline__ void stage_box(T* dst, const T* __restrict__ m, const T* __restrict__ u, bool blend, T r,
+                                          T omr, int xs, int ys, int zs, int ex, int ey, int ez) {
+    for (int e = threadIdx.x; e < W * H * D; e += kTileThreads) {
+        const int ix = e % W, rr = e / W, iy = rr % H, iz = rr / H;
+        const long long gi = clampi(xs + ix, 0, ex - 1) +
+                             (long long)ex * (clampi(ys + iy, 0, ey - 1) + (long long)ey * clampi(zs + iz, 0, ez - 1));
+        if (blend) dst[e] = r * m[gi] + omr * u[gi];
+        else cp_async_elem<sizeof(T)>(dst + e, m + gi);
+    }
+}
+
+// staged tables of one axis: value of table k at axis index i (i in [lo-2, lo+len+2])
+template <class T, int S> struct TabSlice {
+    const T* t;
+    int lo;
+    __device__ __forceinline__ T operator()(int k, int i) const { return t[k * S + (i - lo + 2)]; }
+};
+
+// viscous flux-form Laplacian of the impulse at a face of component A from its staged box (strides 1, MW,
+// MW*MH), wall and lid fluxes, then the RK combination with the inviscid term L (backend.cu:289-329)
+template <int A, class T, int MW, int MH, class TS0, class TS1, class TS2>
+__device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* mb, T wall, const StageConst& sc, T dt,
+                                             T lidv, int x, int y, int z, int i, T L, const TS0& ts0, const TS1& ts1,
+                                             const TS2& ts2) {
+    const Params& p = a.p;
+    const int q[3] = {x, y, z};
+    const int n[3] = {p.nx, p.ny, p.nz};
+    constexpr int stride[3] = {1, MW, MW * MH};
+    const T cc = mb[0];
+    T lap = T(0);
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+        const auto tb = [&](int k, int idx) { return t == 0 ? ts0(k, idx) : t == 1 ? ts1(k, idx) : ts2(k, idx); };
+        const int s = stride[t];
+        if (t == A) {
+            lap = lap + ((mb[s] - cc) * tb(kInvW, q[t]) - (cc - mb[-s]) * tb(kInvW, q[t] - 1)) * tb(kInvSp, q[t]);
+            continue;
+        }
+        T hi = q[t] < n[t] - 1 ? (mb[s] - cc) * tb(kInvSp, q[t] + 1) : T(0);
+        T lo = q[t] > 0 ? (cc - mb[-s]) * tb(kInvSp, q[t]) : T(0);
+        if (q[t] == 0) lo = wall * tb(kInvSp, 0);
+        if (q[t] == n[t] - 1) {
+            if (t == Y) {
+                const T U = A == X ? lidv * a.g.lid_u[x + (p.nx + 1) * z] : T(0);
+                hi = (U - wall) * tb(kInvSp, n[Y]);
+            } else {
+                hi = -wall * tb(kInvSp, n[t]);
+            }
+        }
+        lap = lap + (hi - lo) * tb(kInvW, q[t]);
+    }
+    T val = cc + dt * (a.nu * lap + L);
+    if (a.stage > 0) val = T(sc.a0) * a.m0[A][i] + T(sc.b) * val;
+    return val;
+}
+
+template <class T, int TY, int TZ>
+__global__ void __launch_bounds__(kTileThreads) sweep_tile_kernel(MomentumArgs<T> a) {
+    using G = TileGeom<TY, TZ>;
+    constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
+    constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
+    constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;      // plane strides of the velocity boxes
+    if (a.c->error) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* SU = reinterpret_cast<T*>(smem_raw);
+    T* SV = SU + G::NU;
+    T* SW = SV + G::NV;
+    T* MX = SW + G::NW;
+    T* MY = MX + G::NM;
+    T* MZ = MY + G::NM;
+    T* Kc = MZ + G::NM;
+    T* TXs = Kc + G::NK;
+    T* TYs = TXs + kNumTabs * G::SX;
+    T* TZs = TYs + kNumTabs * G::SY;
+    const Params& p = a.p;
+    const Geo<T>& g = a.g;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    const int o4 = p.o4;
+    const bool blend = a.stage == 0;
+
+    // ---- stage
+    stage_box<T, UW, UH, G::UD>(SU, a.u[X], nullptr, false, T(0), T(0), x0 - 1, y0 - 3, z0 - 3, nx + 1, ny, nz);
+    stage_box<T, VW, VH, G::VD>(SV, a.u[Y], nullptr, false, T(0), T(0), x0 - 3, y0 - 1, z0 - 3, nx, ny + 1, nz);
+    stage_box<T, WW, WH, G::WD>(SW, a.u[Z], nullptr, false, T(0), T(0), x0 - 3, y0 - 3, z0 - 1, nx, ny, nz + 1);
+    stage_box<T, MW, MH, G::MD>(MX, a.m[X], a.u[X], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx + 1, ny, nz);
+    stage_box<T, MW, MH, G::MD>(MY, a.m[Y], a.u[Y], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny + 1, nz);
+    stage_box<T, MW, MH, G::MD>(MZ, a.m[Z], a.u[Z], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny, nz + 1);
+    for (int e = threadIdx.x; e < kNumTabs * (G::SX + G::SY + G::SZ); e += kTileThreads) {
+        int k, i, axis, len, lo;
+        if (e < kNumTabs * G::SX) { axis = X; k = e / G::SX; i = e % G::SX; len = G::SX; lo = x0; }
+        else if (e < kNumTabs * (G::SX + G::SY)) {
+            const int f = e - kNumTabs * G::SX;
+            axis = Y; k = f / G::SY; i = f % G::SY; len = G::SY; lo = y0;
+        } else {
+            const int f = e - kNumTabs * (G::SX + G::SY);
+            axis = Z; k = f / G::SZ; i = f % G::SZ; len = G::SZ; lo = z0;
+        }
+        const int n = axis == X ? nx : axis == Y ? ny : nz;
+        const int idx = clampi(lo - 2 + i, -2, n + 2);
+        T* dst = axis == X ? TXs : axis == Y ? TYs : TZs;
+        dst[k * len + i] = tab(g, axis, k, idx);
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    const TabSlice<T, G::SX> tX{TXs, x0};
+    const TabSlice<T, G::SY> tY{TYs, y0};
+    const TabSlice<T, G::SZ> tZ{TZs, z0};
+
+    // ---- K = u.m per cell (x0-1+ix, y0-1+iy, z0-1+iz)
+    for (int e = threadIdx.x; e < G::NK; e += kTileThreads) {
+        const int ix = e % (TX + 1), r = e / (TX + 1), iy = r % (TY + 1), iz = r / (TY + 1);
+        const T* u0 = SU + ((iz + 2) * UH + iy + 2) * UW + ix;
+        const T* v0 = SV + ((iz + 2) * VH + iy) * VW + 2 + ix;
+        const T* w0 = SW + (iz * WH + iy + 2) * WW + 2 + ix;
+        const int mi = (iz * MH + iy) * MW + ix;
+        Kc[e] = T(0.5) * ((u0[0] * MX[mi] + u0[1] * MX[mi + 1]) + (v0[0] * MY[mi] + v0[VW] * MY[mi + MW]) +
+                          (w0[0] * MZ[mi] + w0[WP] * MZ[mi + MH * MW]));
+    }
+    __syncthreads();
+
+    const StageConst sc = stage_const(a.stage, a.c);
+    const T dt = (T)a.c->dt;
+    const T lidv = (T)lid_speed(p, sc.tau);
+    const T half = T(0.5), eighth = T(0.125);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto kidx = [&](int ix, int iy, int iz) { return (iz * (TY + 1) + iy) * (TX + 1) + ix; };
+    // stencil weights of an edge between axis indices ia (axis A) and ib (axis B)
+    auto w1 = [&](T okA, T okB, T lA, T lB) { return o4 ? okA * okB * (T(1) + (lA * lB) * eighth) : okA * okB; };
+    auto w3 = [&](T lA, T lB) { return -((lA * lB) * eighth); };
+
+#pragma unroll 1
+    for (int k = 0; k < RPT; k++) {
+        const int row = warp + 8 * k, ry = row % TY, rz = row / TY;
+        const int x = x0 + lane, y = y0 + ry, z = z0 + rz;
+        if (x >= nx || y >= ny || z >= nz) continue;
+        const T* pu = SU + ((rz + 3) * UH + ry + 3) * UW + lane + 1;   // u at x-face x, cells (y, z)
+        const T* pv = SV + ((rz + 3) * VH + ry + 1) * VW + lane + 3;   // v at cell x, y-face y, cell z
+        const T* pw = SW + ((rz + 1) * WH + ry + 3) * WW + lane + 3;   // w at cells (x, y), z-face z
+        const int mo = ((rz + 1) * MH + ry + 1) * MW + lane + 1;        // this cell's lower faces in the impulse boxes
+        const T kc = Kc[kidx(lane + 1, ry + 1, rz + 1)];
+
+        // ---------------- u-face x: z-edges (b = Y, omega_z) and y-edges (b = Z, omega_y)
+        {
+            const int i = fidx<X>(p, x, y, z);
+            if (blend) a.m0_out[X][i] = MX[mo];
+            if (x == 0) a.out[X][i] = T(0);
+            else {
+                const T ok1x = tX(kOk1, x), l1x = tX(kL1, x), l3x = tX(kL3, x), i1x = tX(kInvSp, x), i3x = tX(kInvNd3, x);
+                const T e1l = tX(kEv1Lo, x), e1h = tX(kEv1Hi, x), e3l = tX(kEv3Lo, x), e3h = tX(kEv3Hi, x);
+                // z-edge at y-face e (d = e - y): + w omega_z ev_x(v)
+                auto pz1 = [&](int d) {
+                    const int e = y + d;
+                    const T vl = pv[d * VW - 1], vh = pv[d * VW], ul = pu[(d - 1) * UW], uh = pu[d * UW];
+                    const T wo = w1(ok1x, tY(kOk1, e), l1x, tY(kL1, e)) * ((vh - vl) * i1x - (uh - ul) * tY(kInvSp, e));
+                    return wo * (e1l * vl + e1h * vh);
+                };
+                auto pz3 = [&](int d) {
+                    const int e = y + d;
+                    const T vl = pv[d * VW - 2], vh = pv[d * VW + 1], ul = pu[(d - 2) * UW], uh = pu[(d + 1) * UW];
+                    const T wo = w3(l3x, tY(kL3, e)) * ((vh - vl) * i3x - (uh - ul) * tY(kInvNd3, e));
+                    return wo * (e3l * vl + e3h * vh);
+                };
+                // y-edge at z-face e (d = e - z): - w omega_y ev_x(w)
+                auto py1 = [&](int d) {
+                    const int e = z + d;
+                    const T ul = pu[(d - 1) * UP], uh = pu[d * UP], wl = pw[d * WP - 1], wh = pw[d * WP];
+                    const T wo = w1(tZ(kOk1, e), ok1x, tZ(kL1, e), l1x) * ((uh - ul) * tZ(kInvSp, e) - (wh - wl) * i1x);
+                    return -(wo * (e1l * wl + e1h * wh));
+                };
+                auto py3 = [&](int d) {
+                    const int e = z + d;
+                    const T ul = pu[(d - 2) * UP], uh = pu[(d + 1) * UP], wl = pw[d * WP - 2], wh = pw[d * WP + 1];
+                    const T wo = w3(tZ(kL3, e), l3x) * ((uh - ul) * tZ(kInvNd3, e) - (wh - wl) * i3x);
+                    return -(wo * (e3l * wl + e3h * wh));
+                };
+                T L = half * (pz1(1) + pz1(0)) + half * (py1(1) + py1(0));
+                if (o4) {
+                    const T c3 = tX(kC3, x);
+                    L = L + c3 * (pz3(2) + pz3(-1));
+                    L = L + c3 * (py3(2) + py3(-1));
+                }
+                L = L - (kc - Kc[kidx(lane, ry + 1, rz + 1)]) * tX(kInvSp, x);
+                a.out[X][i] = viscous_rk_tile<X, T, MW, MH>(a, MX + mo, pu[0], sc, dt, lidv, x, y, z, i, L, tX, tY, tZ);
+            }
+            if (x == nx - 1) {
+                if (blend) a.m0_out[X][i + 1] = MX[mo + 1];
+                a.out[X][i + 1] = T(0);
+            }
+        }
+        // ---------------- v-face y: z-edges (b = X, omega_z) and x-edges (b = Z, omega_x)
+        {
+            const int i = fidx<Y>(p, x, y, z);
+            if (blend) a.m0_out[Y][i] = MY[mo];
+            if (y == 0) a.out[Y][i] = T(0);
+            else {
+                const T ok1y = tY(kOk1, y), l1y = tY(kL1, y), l3y = tY(kL3, y), i1y = tY(kInvSp, y), i3y = tY(kInvNd3, y);
+                const T e1l = tY(kEv1Lo, y), e1h = tY(kEv1Hi, y), e3l = tY(kEv3Lo, y), e3h = tY(kEv3Hi, y);
+                // z-edge at x-face e (d = e - x): - w omega_z ev_y(u)
+                auto pz1 = [&](int d) {
+                    const int e = x + d;
+                    const T vl = pv[d - 1], vh = pv[d], ul = pu[d - UW], uh = pu[d];
+                    const T wo = w1(tX(kOk1, e), ok1y, tX(kL1, e), l1y) * ((vh - vl) * tX(kInvSp, e) - (uh - ul) * i1y);
+                    return -(wo * (e1l * ul + e1h * uh));
+                };
+                auto pz3 = [&](int d) {
+                    const int e = x + d;
+                    const T vl = pv[d - 2], vh = pv[d + 1], ul = pu[d - 2 * UW], uh = pu[d + UW];
+                    const T wo = w3(tX(kL3, e), l3y) * ((vh - vl) * tX(kInvNd3, e) - (uh - ul) * i3y);
+                    return -(wo * (e3l * ul + e3h * uh));
+                };
+                // x-edge at z-face e (d = e - z): + w omega_x ev_y(w)
+                auto px1 = [&](int d) {
+                    const int e = z + d;
+                    const T wl = pw[d * WP - WW], wh = pw[d * WP], vl = pv[(d - 1) * VP], vh = pv[d * VP];
+                    const T wo = w1(ok1y, tZ(kOk1, e), l1y, tZ(kL1, e)) * ((wh - wl) * i1y - (vh - vl) * tZ(kInvSp, e));
+                    return wo * (e1l * wl + e1h * wh);
+                };
+                auto px3 = [&](int d) {
+                    const int e = z + d;
+                    const T wl = pw[d * WP - 2 * WW], wh = pw[d * WP + WW], vl = pv[(d - 2) * VP], vh = pv[(d + 1) * VP];
+                    const T wo = w3(l3y, tZ(kL3, e)) * ((wh - wl) * i3y - (vh - vl) * tZ(kInvNd3, e));
+                    return wo * (e3l * wl + e3h * wh);
+                };
+                T L = half * (pz1(1) + pz1(0)) + half * (px1(1) + px1(0));
+                if (o4) {
+                    const T c3 = tY(kC3, y);
+                    L = L + c3 * (pz3(2) + pz3(-1));
+                    L = L + c3 * (px3(2) + px3(-1));
+                }
+                L = L - (kc - Kc[kidx(lane + 1, ry, rz + 1)]) * tY(kInvSp, y);
+                a.out[Y][i] = viscous_rk_tile<Y, T, MW, MH>(a, MY + mo, pv[0], sc, dt, lidv, x, y, z, i, L, tX, tY, tZ);
+            }
+            if (y == ny - 1) {
+                if (blend) a.m0_out[Y][i + nx] = MY[mo + MW];
+                a.out[Y][i + nx] = T(0);
+            }
+        }
+        // ---------------- w-face z: x-edges (b = Y, omega_x) and y-edges (b = X, omega_y)
+        {
+            const int i = fidx<Z>(p, x, y, z);
+            if (blend) a.m0_out[Z][i] = MZ[mo];
+            if (z == 0) a.out[Z][i] = T(0);
+            else {
+                const T ok1z = tZ(kOk1, z), l1z = tZ(kL1, z), l3z = tZ(kL3, z), i1z = tZ(kInvSp, z), i3z = tZ(kInvNd3, z);
+                const T e1l = tZ(kEv1Lo, z), e1h = tZ(kEv1Hi, z), e3l = tZ(kEv3Lo, z), e3h = tZ(kEv3Hi, z);
+                // x-edge at y-face e (d = e - y): - w omega_x ev_z(v)
+                auto px1 = [&](int d) {
+                    const int e = y + d;
+                    const T wl = pw[(d - 1) * WW], wh = pw[d * WW], vl = pv[d * VW - VP], vh = pv[d * VW];
+                    const T wo = w1(tY(kOk1, e), ok1z, tY(kL1, e), l1z) * ((wh - wl) * tY(kInvSp, e) - (vh - vl) * i1z);
+                    return -(wo * (e1l * vl + e1h * vh));
+                };
+                auto px3 = [&](int d) {
+                    const int e = y + d;
+                    const T wl = pw[(d - 2) * WW], wh = pw[(d + 1) * WW], vl = pv[d * VW - 2 * VP], vh = pv[d * VW + VP];
+                    const T wo = w3(tY(kL3, e), l3z) * ((wh - wl) * tY(kInvNd3, e) - (vh - vl) * i3z);
+                    return -(wo * (e3l * vl + e3h * vh));
+                };
+                // y-edge at x-face e (d = e - x): + w omega_y ev_z(u)
+                auto py1 = [&](int d) {
+                    const int e = x + d;
+                    const T ul = pu[d - UP], uh = pu[d], wl = pw[d - 1], wh = pw[d];
+                    const T wo = w1(ok1z, tX(kOk1, e), l1z, tX(kL1, e)) * ((uh - ul) * i1z - (wh - wl) * tX(kInvSp, e));
+                    return wo * (e1l * ul + e1h * uh);
+                };
+                auto py3 = [&](int d) {
+                    const int e = x + d;
+                    const T ul = pu[d - 2 * UP], uh = pu[d + UP], wl = pw[d - 2], wh = pw[d + 1];
+                    const T wo = w3(l3z, tX(kL3, e)) * ((uh - ul) * i3z - (wh - wl) * tX(kInvNd3, e));
+                    return wo * (e3l * ul + e3h * uh);
+                };
+                T L = half * (px1(1) + px1(0)) + half * (py1(1) + py1(0));
+                if (o4) {
+                    const T c3 = tZ(kC3, z);
+                    L = L + c3 * (px3(2) + px3(-1));
+                    L = L + c3 * (py3(2) + py3(-1));
+                }
+                L = L - (kc - Kc[kidx(lane + 1, ry + 1, rz)]) * tZ(kInvSp, z);
+                a.out[Z][i] = viscous_rk_tile<Z, T, MW, MH>(a, MZ + mo, pw[0], sc, dt, lidv, x, y, z, i, L, tX, tY, tZ);
+            }
+            if (z == nz - 1) {
+                if (blend) a.m0_out[Z][i + nx * ny] = MZ[mo + MW * MH];
+                a.out[Z][i + nx * ny] = T(0);
+            }
+        }
+    }
+}
+
+}  // namespace cavity

@@ -72,3 +72,20 @@ def kick_noise(shapes, seed, number):
     """Standard-normal kick noise on u, v, w for kick `number` (1-based)."""
     rng = np.random.default_rng(seed + 1000 + number - 1)
     return [rng.standard_normal(shapes[c]) for c in 'uvw']
+
+
+def ensemble_cases(count=256, seed=0, sizes=(24, 32, 48, 64), re_range=(100.0, 2000.0), noise=1e-3):
+    """C4: `count` cavities, sizes drawn uniformly from `sizes`, half uniform and half stretched (beta 1.5),
+    Re log-uniform in `re_range`, independent noise seeds; mixed form, CFL 0.5."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for k in range(count):
+        n = int(rng.choice(sizes))
+        re = float(np.exp(rng.uniform(np.log(re_range[0]), np.log(re_range[1]))))
+        beta = 1.5 if k % 2 else None
+        cases.append(dict(name=f'cavity{k:03d}', settings=settings(n, re, beta=beta, cfl=0.5), noise=noise, seed=k,
+                          precision='mixed'))
+    return cases
+
+
+C4 = dict(name='c4_ensemble256', steps=1000, cases=ensemble_cases)

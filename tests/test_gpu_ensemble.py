@@ -1,0 +1,29 @@
+"""Several cavities advanced together (concurrent streams) give each cavity exactly the result it has alone."""
+import numpy as np
+import pytest
+
+from les_impulse3d_64_b200 import workloads
+from les_impulse3d_64_b200.ensemble import Ensemble
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ensemble_matches_alone():
+    cases = workloads.ensemble_cases(count=6, seed=3, sizes=(12, 16, 24), re_range=(100.0, 2000.0))
+    for k, c in enumerate(cases):
+        c['precision'] = 'fp64' if k % 2 else 'mixed'
+    ens = Ensemble(cases)
+    try:
+        ens.advance(5, chunk=3)
+        together = [ens.fields(i) for i in range(len(cases))]
+    finally:
+        ens.close()
+    for i in (0, 3, 5):
+        alone = Ensemble([cases[i]])
+        try:
+            alone.advance(5, chunk=1)
+            f = alone.fields(0)
+        finally:
+            alone.close()
+        for k in f:
+            assert np.array_equal(f[k], together[i][k]), (i, k)
