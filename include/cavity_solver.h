@@ -105,6 +105,13 @@ int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
  * nx*ny*nz intermediates on that stream, and returns when phi is updated. */
 int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                     const double* inv_lambda, const double* r, double* phi, void* stream);
+/* The mixed form's FDM pass on the tcgen05 tensor cores, on caller-provided device arrays: the operation of
+ * backend.cu:801-814 with its scaling of r to rms 1, S and 1/lambda rounded to float (backend.cu:766-786)
+ * and fp32 transforms, each computed as three TF32 products (3xTF32).  Same arguments as cavity_fdm_pass
+ * (st is checked but not read: S^T is formed from s).  nx must be a multiple of 4.  Allocates its
+ * intermediates on `stream` and returns when phi is updated. */
+int cavity_fdm_pass_tf32(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                         const double* inv_lambda, const double* r, double* phi, void* stream);
 /* cavity_fdm_pass without any device allocation (no counterpart in the reference).  For callers that must
  * not allocate device memory themselves or through this library: a host whose device memory is all owned
  * by its own pool allocator, or a process running with the device nearly full, where a cudaMalloc would

@@ -32,6 +32,7 @@ enum ErrorCode : int {
     kRhsNaN = 2,           // backend.cu:820
     kResidualNaN = 3,      // backend.cu:838
     kNotConverged = 4,     // backend.cu:840-844
+    kDeviceWait = 5,       // a bounded wait on the tensor cores ran out (no counterpart in the reference)
 };
 enum Counter : int { kCntDiv = 0, kCntRes, kCntFinish, kCntCfl, kNumCounters };
 

@@ -22,6 +22,7 @@
 #include "cavity_solver.h"
 #include "kernels.cuh"
 #include "fdm.cuh"
+#include "tc_gemm.cuh"
 #include "sweep.cuh"
 #include "sweep_tile.cuh"
 #include "outputs.cuh"
@@ -110,6 +111,12 @@ public:
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
         setup_params();
+        {
+            // mixed form: FDM transforms on the tcgen05 tensor cores (3xTF32) unless CAVITY_FDM=dmma; their float4
+            // row loads need nx % 4 == 0, otherwise the FP64 DMMA transforms run
+            const char* f = std::getenv("CAVITY_FDM");
+            tc_fdm_ = sizeof(T) == 4 && nx_ % 4 == 0 && !(f && std::string(f) == "dmma");
+        }
         allocate();
         upload_tables();
         build_graphs();
@@ -395,7 +402,14 @@ private:
         int sms = 148, dev = 0;
         check(cudaGetDevice(&dev));
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        sms_ = sms;
         cell_blocks_ = (unsigned int)std::min<long long>(blocks_for(n_cell_), 4LL * sms);
+        if (tc_fdm_) {
+            inv_lambda_f_ = arena_.alloc<float>(n_cell_);
+            const int n[3] = {nx_, ny_, nz_};
+            for (int a = 0; a < 3; a++)
+                for (int i = 0; i < 4; i++) img_[a][i] = arena_.alloc<float>(basis_image_floats(n[a], n[a]));
+        }
         partial_ = arena_.alloc<double>(8 * partial_blocks_);
         ctrl_ = arena_.alloc<Control>(1);
         slots_ = arena_.alloc<double>(kNumSlots);
@@ -458,6 +472,20 @@ private:
                         zero ? 0.0 : 1.0 / (e[2].lambda[z] + e[1].lambda[y] + e[0].lambda[x]);
                 }
         check(cudaMemcpy(inv_lambda_, inv.data(), sizeof(double) * n_cell_, cudaMemcpyHostToDevice));
+        if (tc_fdm_) {
+            // float S and 1/lambda as the reference keeps them (backend.cu:766-786), S split into hi/lo TF32
+            // images of its rows (img 0, 1) and of its columns = rows of S^T (img 2, 3)
+            convert_kernel<double, float><<<blocks_for(n_cell_), kThreads, 0, stream_>>>(inv_lambda_, inv_lambda_f_,
+                                                                                          n_cell_);
+            tcop_.nx = nx_; tcop_.ny = ny_; tcop_.nz = nz_;
+            tcop_.inv_lambda = inv_lambda_f_;
+            for (int a = 0; a < 3; a++) {
+                launch_basis_image(stream_, S_[a], ax_[a].n, 0, img_[a][0], img_[a][1]);
+                launch_basis_image(stream_, S_[a], ax_[a].n, 1, img_[a][2], img_[a][3]);
+                for (int i = 0; i < 4; i++) tcop_.img[a][i] = img_[a][i];
+            }
+            check(cudaGetLastError());
+        }
         fdm_.nx = nx_; fdm_.ny = ny_; fdm_.nz = nz_;
         for (int a = 0; a < 3; a++) { fdm_.s[a] = S_[a]; fdm_.st[a] = ST_[a]; }
         fdm_.inv_lambda = inv_lambda_;
@@ -483,6 +511,7 @@ private:
         case kVelocityNaN: fail("velocity is NaN/inf: the solution has blown up");
         case kRhsNaN: fail("pressure solve: right-hand side is NaN/inf (the run has blown up)");
         case kResidualNaN: fail("pressure solve: residual is NaN/inf");
+        case kDeviceWait: fail("pressure solve: a tensor-core transform timed out waiting for its MMAs");
         case kNotConverged:
             std::snprintf(msg, sizeof msg, "pressure solve: residual %.2e > FDM_RTOL after %d passes", hc_.error_value,
                           hc_.error_passes);
@@ -580,8 +609,13 @@ private:
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
-        launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h);
+        if (tc_fdm_) launch_tc_pass(st, phi, h, use_h);
+        else launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h);
         launch_residual(st, phi, h, use_h);
+    }
+    void launch_tc_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
+        launch_tc_fdm_pass(st, tcop_, res_, rhs_, phi, reinterpret_cast<float*>(t1_), reinterpret_cast<float*>(t2_),
+                           ctrl_, h, use_h, sms_);
     }
     void launch_finish(cudaStream_t st, T* const m[3], T* const u_out[3], double* phi_out, bool step_mode, int stage,
                        bool last) {
@@ -670,6 +704,7 @@ private:
             if (tile_sweep_)
                 check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::template smem_bytes<T>()));
+            if (tc_fdm_) check(tc_transform_prepare());
         }
         for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
         const char* env = std::getenv("CAVITY_GRAPHS");
@@ -733,6 +768,11 @@ private:
     double *phi0_, *praw_, *base_, *rhs_, *res_, *hist_[4], *t1_, *t2_, *inv_lambda_;
     double *S_[3], *ST_[3];
     FdmOperands fdm_;
+    bool tc_fdm_ = false;              // mixed form: tcgen05 transforms
+    int sms_ = 148;
+    float* inv_lambda_f_ = nullptr;
+    float* img_[3][4] = {};            // per axis: S rows hi, lo; S^T rows hi, lo (basis images)
+    TcFdmOperands tcop_ = {};
     double* partial_;
     long long partial_blocks_;
     unsigned int cell_blocks_ = 1;     // grid of the grid-stride cell kernels: at most 4 CTAs per SM
@@ -760,8 +800,65 @@ static long long estimate_bytes(const CavityConfig& c, int precision) {
     const long long faces = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1);
     const long long fb = precision == 0 ? 8 : 4;
     const long long maxface = std::max((nx + 1) * ny * nz, nx * ny * (nz + 1));
+    const long long tc = precision == 1 && nx % 4 == 0
+                             ? 4 * cells + 4 * 4 * (cavity::basis_image_floats((int)nx, (int)nx) +
+                                                    cavity::basis_image_floats((int)ny, (int)ny) +
+                                                    cavity::basis_image_floats((int)nz, (int)nz))
+                             : 0;
     return 7 * faces * fb + 16 * cells * 8 + 2 * 8 * maxface + 4 * std::max(maxface, 2 * cells) +
-           2 * 8 * (nx * nx + ny * ny + nz * nz) + 64 * (maxface / 256 + 8) + (1 << 20);
+           2 * 8 * (nx * nx + ny * ny + nz * nz) + 64 * (maxface / 256 + 8) + tc + (1 << 20);
+}
+
+// One FDM pass of the mixed form on the tensor cores on caller-provided device arrays, with the reference's
+// scaling of r to rms 1 and float S and 1/lambda (backend.cu:766-814); every intermediate is allocated on the
+// stream.
+static void fdm_pass_tf32(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                          const double* inv_lambda, const double* r, double* phi, cudaStream_t stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || nx > 1024 || ny > 1024 || nz > 1024) fail("fdm pass: 1 <= nx, ny, nz <= 1024");
+    if (nx % 4) fail("fdm pass (tensor cores): nx must be a multiple of 4");
+    if (!inv_lambda || !r || !phi) fail("fdm pass: null pointer");
+    for (int a = 0; a < 3; a++)
+        if (!s[a] || !st[a]) fail("fdm pass: null eigenbasis");
+    const long long n = (long long)nx * ny * nz;
+    const int dims[3] = {nx, ny, nz};
+    int dev = 0, sms = 148;
+    check(cudaGetDevice(&dev));
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    check(tc_transform_prepare());
+    std::vector<void*> owned;
+    auto alloc = [&](size_t bytes) {
+        void* p = nullptr;
+        check(cudaMallocAsync(&p, bytes, stream));
+        owned.push_back(p);
+        return p;
+    };
+    float* t1 = (float*)alloc(sizeof(float) * n);
+    float* t2 = (float*)alloc(sizeof(float) * n);
+    float* invf = (float*)alloc(sizeof(float) * n);
+    Control* c = (Control*)alloc(sizeof(Control));
+    TcFdmOperands op;
+    op.nx = nx; op.ny = ny; op.nz = nz;
+    op.inv_lambda = invf;
+    for (int a = 0; a < 3; a++) {
+        float* img[4];
+        for (int i = 0; i < 4; i++) img[i] = (float*)alloc(sizeof(float) * basis_image_floats(dims[a], dims[a]));
+        launch_basis_image(stream, s[a], dims[a], 0, img[0], img[1]);
+        launch_basis_image(stream, s[a], dims[a], 1, img[2], img[3]);
+        for (int i = 0; i < 4; i++) op.img[a][i] = img[i];
+    }
+    const Control hc = standalone_fdm_control();
+    check(cudaMemcpyAsync(c, &hc, sizeof hc, cudaMemcpyHostToDevice, stream));
+    control_norm_kernel<<<1, kThreads, 0, stream>>>(r, n, c);
+    convert_kernel<double, float><<<blocks_for(n), kThreads, 0, stream>>>(inv_lambda, invf, n);
+    launch_tc_fdm_pass(stream, op, r, nullptr, phi, t1, t2, c, 0, false, sms);
+    const cudaError_t launched = cudaGetLastError();
+    Control out;
+    const cudaError_t copied = cudaMemcpyAsync(&out, c, sizeof out, cudaMemcpyDeviceToHost, stream);
+    for (void* p : owned) check(cudaFreeAsync(p, stream));
+    check(launched);
+    check(copied);
+    check(cudaStreamSynchronize(stream));
+    if (out.error == kDeviceWait) fail("fdm pass (tensor cores): a transform timed out waiting for its MMAs");
 }
 
 // One FDM pass on caller-provided device arrays; the two intermediates are allocated on the stream.
@@ -958,6 +1055,10 @@ int cavity_kernels_per_step(const CavitySolver* s, int passes) { return s && s->
 int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                     const double* inv_lambda, const double* r, double* phi, void* stream) {
     return safely([&] { cavity::fdm_pass(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
+}
+int cavity_fdm_pass_tf32(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
+                         const double* inv_lambda, const double* r, double* phi, void* stream) {
+    return safely([&] { cavity::fdm_pass_tf32(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
 }
 int cavity_fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                             const double* inv_lambda, const double* r, double* phi, void* stream) {

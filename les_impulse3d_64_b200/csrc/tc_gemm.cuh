@@ -1,0 +1,565 @@
+// tc_gemm.cuh - the FDM transforms of the mixed form on the 5th-generation tensor cores (tcgen05), FP32-accurate
+// through the 3xTF32 split: every fp32 operand x is written as hi + lo with hi = x rounded to TF32 and lo = x - hi,
+// and a product is accumulated as a_lo b_hi + a_hi b_lo + a_hi b_hi in FP32 (the a_lo b_lo term is below fp32
+// rounding).  This is the mixed form's counterpart of the reference's FP32 SGEMM transforms (backend.cu:792-814);
+// the FP64 form keeps its FP64 DMMA transforms (fdm.cuh).
+//
+// One launch computes C[b] (M x N) = A[b] (M x K) * B[b] (K x N) for one of the six transforms of a pass.
+// One operand is the field (fp32 t1/t2, or the fp64 residual scaled by 1/rms in the first transform) and the
+// other a basis S or S^T of one axis, pre-split at set-up into hi/lo "images" laid out in shared-memory order.
+//
+//  * field_is_a = 1 (the x transforms): A = field rows [m][k], B = basis image.
+//  * field_is_a = 0 (the y and z transforms): A = basis image, B = field [k][n] (n contiguous), transposed into
+//    the K-major layout on its way to shared memory.
+//
+// Both operands sit in shared memory in the K-major, non-swizzled canonical layout.  A CTA of 128 threads owns a
+// 128 x BN tile of C held in TMEM (128 lanes x BN fp32 columns).  K runs in panels of 32 through two
+// shared-memory stages: the threads load panel p+1 (field values split into hi/lo, one 16-byte shared store per
+// 4 consecutive k; cp.async copies of the basis image) while the tensor core works on panel p.  One
+// thread issues the tcgen05.mma.cta_group::1.kind::tf32 instructions (M = 128, N = BN, K = 8) and commits each
+// panel to that stage's mbarrier.  Every mbarrier wait is bounded: on time-out the kernel records
+// kDeviceWait in the control block, frees its TMEM and returns.  Only this kernel allocates TMEM, and the
+// shared memory of a CTA (>= 80 KB) keeps at most 2 CTAs of <= 128 columns on an SM, below its 512 columns.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace cavity {
+
+constexpr int kTcThreads = 128;
+constexpr int kTcKC = 32;                 // K panel
+constexpr int kTcRows = 128;              // M of the tile (TMEM lanes)
+
+// ---------------------------------------------------------------- PTX wrappers
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, no swizzle: start address, LBO = byte distance between core matrices adjacent
+// along K, SBO = between core matrices adjacent along M/N, version 1 (sm_100), layout type 0 (no swizzle)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+// instruction descriptor of kind::tf32 with fp32 accumulation; a_mn / b_mn = 1 would select MN-major operands
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N, int a_mn, int b_mn) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase of parity `parity` of an mbarrier to complete; false on time-out (~0.3 s)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (long it = 0; it < (1L << 22); it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_alloc(uint32_t* result, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(result)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// 16 consecutive fp32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+}
+__device__ __forceinline__ void cp_async16_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void st_shared4(uint32_t addr, float a, float b, float c, float d) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
+
+// ---------------------------------------------------------------- 3xTF32 split
+// hi = x rounded to the nearest TF32 value (10 explicit mantissa bits), lo = x - hi (exact in fp32).  Inf and NaN
+// pass through hi so that a blown-up field still shows in the residual.
+__host__ __device__ inline void tf32_split(float x, float& hi, float& lo) {
+    uint32_t bits;
+    memcpy(&bits, &x, 4);
+    if ((bits & 0x7F800000u) == 0x7F800000u) { hi = x; lo = 0.0f; return; }
+    const uint32_t hb = (bits + 0x1000u) & 0xFFFFE000u;
+    memcpy(&hi, &hb, 4);
+    lo = x - hi;
+}
+
+// ---------------------------------------------------------------- layouts
+// K-major, no swizzle: core matrices of 8 rows x 16 bytes (4 elements along K); K-adjacent cores 128 bytes apart
+// (LBO), 8-row groups kTcKC/4 * 128 = 1024 bytes apart (SBO).  Byte offset of (row r, k) in a 32-wide K panel:
+__host__ __device__ constexpr int kmajor_off(int r, int k) {
+    return ((r >> 3) * (kTcKC / 4) + (k >> 2)) * 128 + (r & 7) * 16 + (k & 3) * 4;
+}
+constexpr uint32_t kKmajorLBO = 128, kKmajorSBO = (kTcKC / 4) * 128;
+
+// A basis image holds the hi (or lo) parts of a matrix with `rows` rows and k columns, rows rounded up to 128 (R)
+// and columns to 32, zero-padded, panel by panel: panel p is the K-major shared-memory image of rows 0..R-1 and
+// columns 32p..32p+31, so that rows [r0, r0 + n) of panel p are the n * 128 contiguous bytes from byte
+// (p * R + r0) * 128.  Element (r, k) is at float (k / 32) * R * 32 + kmajor_off(r, k % 32) / 4.
+__host__ __device__ constexpr int basis_image_rows(int rows) { return (rows + kTcRows - 1) / kTcRows * kTcRows; }
+__host__ __device__ constexpr long long basis_image_floats(int rows, int k) {
+    return (long long)basis_image_rows(rows) * ((k + kTcKC - 1) / kTcKC * kTcKC);
+}
+__host__ __device__ constexpr long long basis_image_index(int R, int r, int k) {
+    return (long long)(k / kTcKC) * R * kTcKC + kmajor_off(r, k % kTcKC) / 4;
+}
+
+enum TcEpilogue : int { kTcStore = 0, kTcScaleInvLambda = 1, kTcAccumulate = 2 };
+
+struct TcTransformArgs {
+    int M, N, K;                   // per batch entry
+    int field_is_a;
+    const float* field;            // fp32 field, or
+    const double* field64;         // fp64 field scaled by 1/rms on load (first transform of a pass)
+    const double* field64_alt;     // replaces field64 when the control block says use_rhs
+    long long field_bstride;       // batch stride of the field (elements)
+    int field_ld;                  // row pitch of the field (elements)
+    const float* basis_hi;         // images (see basis_image_floats)
+    const float* basis_lo;
+    int basis_rows;                // R of the images
+    float* out;
+    long long out_bstride;
+    int out_ld;
+    const float* inv_lambda;       // kTcScaleInvLambda: indexed like out
+    double* phi;                   // kTcAccumulate: phi[i] = (reset ? 0 : phi[i]) + rms * C (indexed like out)
+    int epilogue;
+    double n_cell;                 // rms = sqrt(|r|^2 / n_cell)
+    const Control* c;
+    int* error;                    // where a timed-out wait is recorded (the control block's error word)
+    cudaGraphConditionalHandle handle;
+    int clear_condition;
+};
+
+template <int BN> struct TcSmem {
+    static constexpr int kA = kTcRows * kTcKC * 4;      // bytes of one A panel part (hi or lo)
+    static constexpr int kB = BN * kTcKC * 4;
+    static constexpr int kStage = 2 * kA + 2 * kB;
+    static constexpr int kBytes = 2 * kStage;
+};
+
+// Work item e of an A panel (128 rows x 8 groups of 4 k): the 8 lanes of a quarter-warp take 8 consecutive rows at
+// one k group, so that their 16-byte shared stores fill one 128-byte row of core matrices without bank conflicts,
+// and a warp's 4 quarters take 4 consecutive k groups, so that it reads 64 contiguous bytes of each of its rows.
+__device__ __forceinline__ void fa_item(int e, int& r, int& k4) {
+    const int hi = e >> 5;
+    r = (e & 7) + 8 * (hi >> 1);
+    k4 = ((e >> 3) & 3) + 4 * (hi & 1);
+}
+
+// The field side of a K panel in registers: FA (field is A) = 128 rows x 32 k, float4 (or two double2 when the
+// source is the fp64 residual) per 4 consecutive k; otherwise 32 k x BN n, as (n, 4 consecutive k) quadruples.
+template <int BN, int FA, int F64> struct FieldPanel {
+    static constexpr int kSlots = FA ? kTcRows * kTcKC / 4 / kTcThreads : BN * kTcKC / 4 / kTcThreads;
+    float4 v[F64 ? 1 : kSlots];
+    double2 d[F64 ? 2 * kSlots : 1];
+};
+
+// grid: (N / BN tiles, M / 128 tiles, batch).  FA: the field is operand A (x transforms); F64: the field is the
+// fp64 residual, scaled by 1/rms (first transform of a pass).
+template <int BN, int FA, int F64>
+__global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArgs g) {
+    using L = TcSmem<BN>;
+    using P = FieldPanel<BN, FA, F64>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    if (g.clear_condition && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+        cudaGraphSetConditional(g.handle, 0u);
+    // the control block is read while TMEM and the barriers are set up
+    const Control* c = g.c;
+    const int err = c->error, use_rhs = c->use_rhs, reset = c->reset_phi;
+    const double rhs2 = c->rhs_norm2, res2 = c->res_norm2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+    const int b = blockIdx.z;
+    const int m0 = blockIdx.y * kTcRows, n0 = blockIdx.x * BN;
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t sbase = smem_addr(smem);
+    constexpr uint32_t kCols = BN < 32 ? 32 : BN;
+    if (warp == 0) tmem_alloc(&tmem_base, kCols);
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        failed = 0;
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const double r2 = use_rhs ? rhs2 : res2;
+    if (err || !(r2 > 0)) {                                    // a zero residual: no pass (backend.cu:803-804)
+        if (warp == 0) tmem_dealloc(tmem, kCols);
+        return;
+    }
+    const double rms = sqrt(r2 / g.n_cell);
+    const double inv_rms = 1.0 / rms;
+    // the epilogue's other operand (phi or 1/lambda) comes into L2 while the panels are multiplied
+    if (row < g.M && g.epilogue != kTcStore && !(g.epilogue == kTcAccumulate && reset)) {
+        const long long base = b * g.out_bstride + (long long)row * g.out_ld + n0;
+        const int cnt = min(BN, g.N - n0);
+        const char* q = g.epilogue == kTcAccumulate ? (const char*)(g.phi + base) : (const char*)(g.inv_lambda + base);
+        const int bytes = cnt * (g.epilogue == kTcAccumulate ? 8 : 4);
+        for (int o = 0; o < bytes; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + o));
+    }
+    const float* F = F64 ? nullptr : g.field + b * g.field_bstride;
+    const double* Fd = F64 ? ((use_rhs && g.field64_alt) ? g.field64_alt : g.field64) + b * g.field_bstride : nullptr;
+    const int panels = (g.K + kTcKC - 1) / kTcKC;
+
+    // issue the field loads of panel p (values stay in flight until store_field uses them)
+    auto load_field = [&](P& f, int p) {
+        const int k0 = p * kTcKC;
+#pragma unroll
+        for (int j = 0; j < P::kSlots; j++) {
+            const int e = tid + j * kTcThreads;
+            if (FA) {                                          // (row, 4 consecutive k): see fa_item
+                int r, k4;
+                fa_item(e, r, k4);
+                const int k = k0 + k4 * 4, gm = m0 + r;
+                const bool ok = gm < g.M && k < g.K;
+                const long long gi = (long long)gm * g.field_ld + k;
+                if (F64) {
+                    f.d[2 * j] = ok ? *reinterpret_cast<const double2*>(Fd + gi) : make_double2(0.0, 0.0);
+                    f.d[2 * j + 1] = ok ? *reinterpret_cast<const double2*>(Fd + gi + 2) : make_double2(0.0, 0.0);
+                } else {
+                    f.v[j] = ok ? *reinterpret_cast<const float4*>(F + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            } else {                                           // (n, 4 consecutive k); a warp reads 32 n of a row
+                const int n = e % BN, k = k0 + (e / BN) * 4, gn = n0 + n;
+                const float* src = F + (long long)k * g.field_ld + gn;
+                const long long ld = g.field_ld;
+                const bool okn = gn < g.N;
+                f.v[j] = make_float4(okn && k < g.K ? src[0] : 0.f, okn && k + 1 < g.K ? src[ld] : 0.f,
+                                     okn && k + 2 < g.K ? src[2 * ld] : 0.f, okn && k + 3 < g.K ? src[3 * ld] : 0.f);
+            }
+        }
+    };
+    // split panel values into hi/lo and store them in the K-major layout of stage s
+    auto store_field = [&](const P& f, int s) {
+        const uint32_t st = sbase + s * L::kStage + (FA ? 0 : 2 * L::kA);
+        const uint32_t part = FA ? L::kA : L::kB;
+#pragma unroll
+        for (int j = 0; j < P::kSlots; j++) {
+            const int e = tid + j * kTcThreads;
+            float4 x;
+            if (F64)
+                x = make_float4((float)(f.d[2 * j].x * inv_rms), (float)(f.d[2 * j].y * inv_rms),
+                                (float)(f.d[2 * j + 1].x * inv_rms), (float)(f.d[2 * j + 1].y * inv_rms));
+            else
+                x = f.v[F64 ? 0 : j];
+            int r, k4;
+            if (FA) fa_item(e, r, k4);
+            else { r = e % BN; k4 = e / BN; }
+            const uint32_t off = kmajor_off(r, k4 * 4);
+            float h0, l0, h1, l1, h2, l2, h3, l3;
+            tf32_split(x.x, h0, l0);
+            tf32_split(x.y, h1, l1);
+            tf32_split(x.z, h2, l2);
+            tf32_split(x.w, h3, l3);
+            st_shared4(st + off, h0, h1, h2, h3);
+            st_shared4(st + part + off, l0, l1, l2, l3);
+        }
+    };
+    // the basis side of panel p into stage s: rows [row0, row0 + rows) of the images, contiguous bytes
+    auto copy_basis = [&](int p, int s) {
+        const uint32_t st = sbase + s * L::kStage;
+        constexpr int rows = FA ? BN : kTcRows;
+        const int row0 = FA ? n0 : m0;
+        const uint32_t dst = FA ? st + 2 * L::kA : st;
+        constexpr uint32_t part = FA ? L::kB : L::kA;
+        const long long src = ((long long)p * g.basis_rows + row0) * kTcKC;      // floats
+        constexpr int chunks = rows * kTcKC / 4;                                  // 16-byte pieces per part
+#pragma unroll
+        for (int e = tid; e < chunks; e += kTcThreads) {
+            cp_async16(dst + e * 16, g.basis_hi + src + e * 4);
+            cp_async16(dst + part + e * 16, g.basis_lo + src + e * 4);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+
+    const uint32_t idesc = umma_idesc_tf32(kTcRows, BN, 0, 0);
+    // panel p: the loads of panel p+1 go out first and stay in flight while panel p (loaded one step earlier
+    // into `cur`) is split, stored and multiplied.  Two register sets alternate (the loop is unrolled by two),
+    // so no register copy ever waits on a load.  Returns false when a bounded wait ran out.
+    auto panel = [&](int p, const P& cur, P& next) -> bool {
+        const int s = p & 1;
+        if (p + 1 < panels) load_field(next, p + 1);
+        store_field(cur, s);                                  // stage s is free: MMA(p-2) finished before basis(p)
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // basis(p) has landed
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t st = sbase + s * L::kStage;
+            const uint32_t a_hi = st, a_lo = st + L::kA, b_hi = st + 2 * L::kA, b_lo = b_hi + L::kB;
+#pragma unroll
+            for (int ks = 0; ks < kTcKC / 8; ks++) {                         // 8 k = two core matrices = 256 B
+                const uint64_t ah = umma_desc(a_hi + ks * 256, kKmajorLBO, kKmajorSBO);
+                const uint64_t al = umma_desc(a_lo + ks * 256, kKmajorLBO, kKmajorSBO);
+                const uint64_t bh = umma_desc(b_hi + ks * 256, kKmajorLBO, kKmajorSBO);
+                const uint64_t bl = umma_desc(b_lo + ks * 256, kKmajorLBO, kKmajorSBO);
+                umma_tf32(tmem, al, bh, idesc, (p > 0 || ks > 0) ? 1u : 0u);
+                umma_tf32(tmem, ah, bl, idesc, 1u);
+                umma_tf32(tmem, ah, bh, idesc, 1u);
+            }
+            umma_commit(&mbar[s]);
+        }
+        if (p + 1 < panels) {
+            // stage s^1 was read by MMA(p-1): wait for it, then bring in the basis of panel p+1
+            if (p >= 1 && !mbar_wait_bounded(&mbar[s ^ 1], ((p - 1) >> 1) & 1)) failed = 1;
+            __syncthreads();
+            if (failed) return false;
+            copy_basis(p + 1, s ^ 1);
+        }
+        return true;
+    };
+    P fa, fb;
+    load_field(fa, 0);
+    copy_basis(0, 0);
+    for (int p = 0; p < panels; p += 2) {
+        if (!panel(p, fa, fb)) break;
+        if (p + 1 < panels && !panel(p + 1, fb, fa)) break;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (!failed && !mbar_wait_bounded(&mbar[(panels - 1) & 1], ((panels - 1) >> 1) & 1)) failed = 1;
+    tc_fence_after();
+    __syncthreads();
+    if (failed) {
+        if (tid == 0) atomicExch(g.error, (int)kDeviceWait);
+        tc_fence_before();
+        __syncthreads();
+        if (warp == 0) tmem_dealloc(tmem, kCols);
+        return;
+    }
+    // epilogue through shared memory (free once every MMA has completed): warp w moves TMEM lanes (tile rows)
+    // 32w..32w+31 into a row-major tile with a pitch of BN + 4 floats (conflict-free 16-byte writes), then
+    // writes its rows back with BN/4 lanes per row, so that every warp access covers contiguous columns.
+    constexpr int kPitch = BN + 4;
+    static_assert(kTcRows * kPitch * 4 <= L::kBytes, "epilogue tile exceeds the stages");
+    float* tile = reinterpret_cast<float*>(smem) + warp * 32 * kPitch;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
+        float* dst = tile + lane * kPitch + c0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            *reinterpret_cast<float4*>(dst + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    }
+    __syncwarp();
+    constexpr int kLanesPerRow = BN / 4, kRowsPerStep = 32 / kLanesPerRow;
+    const int lr = lane / kLanesPerRow, lc = (lane % kLanesPerRow) * 4;
+    const int gcol = n0 + lc;
+#pragma unroll 4
+    for (int r0 = 0; r0 < 32; r0 += kRowsPerStep) {
+        const int rl = r0 + lr, grow = m0 + warp * 32 + rl;
+        if (grow >= g.M || gcol >= g.N) continue;             // N is a multiple of 4: a float4 is all in or out
+        float4 x = *reinterpret_cast<const float4*>(tile + rl * kPitch + lc);
+        const long long idx = b * g.out_bstride + (long long)grow * g.out_ld + gcol;
+        if (g.epilogue == kTcAccumulate) {
+            double2 p0 = make_double2(0.0, 0.0), p1 = make_double2(0.0, 0.0);
+            if (!reset) {
+                p0 = *reinterpret_cast<const double2*>(g.phi + idx);
+                p1 = *reinterpret_cast<const double2*>(g.phi + idx + 2);
+            }
+            p0.x += (double)x.x * rms; p0.y += (double)x.y * rms;
+            p1.x += (double)x.z * rms; p1.y += (double)x.w * rms;
+            *reinterpret_cast<double2*>(g.phi + idx) = p0;
+            *reinterpret_cast<double2*>(g.phi + idx + 2) = p1;
+        } else {
+            if (g.epilogue == kTcScaleInvLambda) {
+                const float4 il = *reinterpret_cast<const float4*>(g.inv_lambda + idx);
+                x.x *= il.x; x.y *= il.y; x.z *= il.z; x.w *= il.w;
+            }
+            *reinterpret_cast<float4*>(g.out + idx) = x;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kCols);
+}
+
+// ---------------------------------------------------------------- host side
+// tile width: the widest of 128 / 64 / 32 columns that still gives one CTA per SM, else 32
+inline int tc_pick_bn(int M, int N, int batch, int sms) {
+    const long long mt = (M + kTcRows - 1) / kTcRows;
+    for (int bn : {128, 64})
+        if ((long long)((N + bn - 1) / bn) * mt * batch >= sms) return bn;
+    return 32;
+}
+// once per device, before any capture: the dynamic shared memory of every instance
+template <int BN> inline cudaError_t tc_prepare_bn() {
+    cudaError_t e = cudaFuncSetAttribute(tc_transform_kernel<BN, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcSmem<BN>::kBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc_transform_kernel<BN, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BN>::kBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc_transform_kernel<BN, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BN>::kBytes);
+    return e;
+}
+inline cudaError_t tc_transform_prepare() {
+    cudaError_t e = tc_prepare_bn<128>();
+    if (e == cudaSuccess) e = tc_prepare_bn<64>();
+    if (e == cudaSuccess) e = tc_prepare_bn<32>();
+    return e;
+}
+template <int BN> inline void launch_tc_bn(cudaStream_t st, const TcTransformArgs& g, dim3 grid) {
+    if (g.field_is_a && g.field64) tc_transform_kernel<BN, 1, 1><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
+    else if (g.field_is_a) tc_transform_kernel<BN, 1, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
+    else tc_transform_kernel<BN, 0, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
+}
+inline void launch_tc_transform(cudaStream_t st, const TcTransformArgs& g, int batch, int sms) {
+    const int bn = tc_pick_bn(g.M, g.N, batch, sms);
+    const dim3 grid((g.N + bn - 1) / bn, (g.M + kTcRows - 1) / kTcRows, batch);
+    if (bn == 128) launch_tc_bn<128>(st, g, grid);
+    else if (bn == 64) launch_tc_bn<64>(st, g, grid);
+    else launch_tc_bn<32>(st, g, grid);
+}
+
+// hi and lo images of S (transpose = 0: image row r = row r of S) or of S^T (transpose = 1: image row r = column r
+// of S) for an n x n row-major double S, rounded to float as the reference keeps S (backend.cu:766-772)
+__global__ void basis_image_kernel(const double* S, int n, int transpose, float* hi, float* lo) {
+    const int R = basis_image_rows(n), Kp = (n + kTcKC - 1) / kTcKC * kTcKC;
+    const long long total = (long long)R * Kp;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / Kp), k = (int)(i % Kp);
+        const float x = r < n && k < n ? (float)(transpose ? S[(size_t)k * n + r] : S[(size_t)r * n + k]) : 0.0f;
+        float h, l;
+        tf32_split(x, h, l);
+        const long long j = basis_image_index(R, r, k);
+        hi[j] = h;
+        lo[j] = l;
+    }
+}
+inline void launch_basis_image(cudaStream_t st, const double* S, int n, int transpose, float* hi, float* lo) {
+    const long long total = basis_image_floats(n, n);
+    basis_image_kernel<<<(unsigned)std::min<long long>((total + 255) / 256, 1024), 256, 0, st>>>(S, n, transpose, hi,
+                                                                                                  lo);
+}
+
+// the operands of a pass on the tensor cores: per axis the images of S (rows; hi, lo) and of S^T (hi, lo), and
+// 1/lambda in float (backend.cu:774-786)
+struct TcFdmOperands {
+    int nx, ny, nz;
+    const float* img[3][4];
+    const float* inv_lambda;
+};
+
+// One pass of backend.cu:801-814 on the tensor cores: r (or r_alt when the control block says use_rhs) scaled
+// to rms 1 in the x transform's loads; t = S_z^T S_y^T (r S_x) in fp32 through t1/t2 (nx*ny*nz floats each);
+// t *= 1/lambda; phi += rms * (S_z S_y t) S_x^T in the last transform's epilogue.  `clear` makes the first launch
+// clear the condition of the enclosing graph while-node `h`.  Needs nx % 4 == 0 (float4 row loads).
+inline void launch_tc_fdm_pass(cudaStream_t st, const TcFdmOperands& op, const double* r, const double* r_alt,
+                               double* phi, float* t1, float* t2, Control* c, cudaGraphConditionalHandle h, bool clear,
+                               int sms) {
+    const int nx = op.nx, ny = op.ny, nz = op.nz, plane = nx * ny;
+    const int n[3] = {nx, ny, nz};
+    TcTransformArgs g = {};
+    g.n_cell = (double)nx * ny * nz;
+    g.c = c;
+    g.error = &c->error;
+    g.inv_lambda = op.inv_lambda;
+    g.phi = phi;
+    g.handle = h;
+    auto basis = [&](int a, bool transpose) {
+        g.basis_hi = op.img[a][transpose ? 2 : 0];
+        g.basis_lo = op.img[a][transpose ? 3 : 1];
+        g.basis_rows = basis_image_rows(n[a]);
+    };
+    // x: rows of the field are the ny*nz x-lines; forward t1 = r S_x, inverse phi += rms * t1 S_x^T
+    auto x_transform = [&](const float* f, bool inverse) {
+        g.M = ny * nz; g.N = nx; g.K = nx; g.field_is_a = 1;
+        g.field = f; g.field64 = inverse ? nullptr : r; g.field64_alt = inverse ? nullptr : r_alt;
+        g.field_bstride = 0; g.field_ld = nx;
+        basis(0, !inverse);
+        g.out = t1; g.out_bstride = 0; g.out_ld = nx;
+        g.epilogue = inverse ? kTcAccumulate : kTcStore;
+        launch_tc_transform(st, g, 1, sms);
+    };
+    // y (each z layer) and z: out = S^T in (forward) or S in (inverse)
+    auto yz_transform = [&](int a, const float* in, float* out, bool inverse, int epi) {
+        const bool y = a == 1;
+        g.M = y ? ny : nz; g.N = y ? nx : plane; g.K = g.M; g.field_is_a = 0;
+        g.field = in; g.field64 = nullptr; g.field64_alt = nullptr;
+        g.field_bstride = y ? plane : 0; g.field_ld = y ? nx : plane;
+        basis(a, !inverse);
+        g.out = out; g.out_bstride = y ? plane : 0; g.out_ld = y ? nx : plane;
+        g.epilogue = epi;
+        launch_tc_transform(st, g, y ? nz : 1, sms);
+    };
+    g.clear_condition = clear;
+    x_transform(nullptr, false);
+    g.clear_condition = 0;
+    yz_transform(1, t1, t2, false, kTcStore);
+    yz_transform(2, t2, t1, false, kTcScaleInvLambda);
+    yz_transform(2, t1, t2, true, kTcStore);
+    yz_transform(1, t2, t1, true, kTcStore);
+    x_transform(t1, true);
+}
+
+// the squared norm of r into the control block of a standalone pass (one block, fixed order)
+__global__ void __launch_bounds__(kThreads) control_norm_kernel(const double* r, long long n, Control* c) {
+    Vec<1> acc;
+    acc.v[0] = 0.0;
+    for (long long i = threadIdx.x; i < n; i += kThreads) acc.v[0] += r[i] * r[i];
+    const Vec<1> tot = block_reduce<1, false>(acc);
+    if (threadIdx.x == 0) {
+        c->res_norm2 = tot.v[0];
+        c->rhs_norm2 = tot.v[0];
+    }
+}
+
+}  // namespace cavity

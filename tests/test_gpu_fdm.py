@@ -59,3 +59,24 @@ def test_fdm_pass_matches_numpy(dims):
     out = call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi)
     ref = fdm_reference(S, r, il, phi)
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize('dims', [(8, 8, 5), (24, 24, 16), (40, 40, 33), (64, 64, 64), (128, 96, 130)])
+def test_fdm_pass_tf32_matches_numpy(dims):
+    """The mixed form's pass on the tensor cores (3xTF32, float S, r scaled to rms 1): the update agrees with
+    the FP64 pass to FP32 level (1e-5 of its largest entry)."""
+    lib = load_library()
+    lib.cavity_last_error.restype = ct.c_char_p
+    S, il, r, phi = random_operands(*dims, seed=sum(dims) + 1)
+    out = call_fdm(lib, 'cavity_fdm_pass_tf32', S, il, r, phi)
+    ref = fdm_reference(S, r, il, phi)
+    upd = ref - phi
+    assert np.abs(out - ref).max() <= 1e-5 * np.abs(upd).max()
+
+
+def test_fdm_pass_tf32_rejects_unaligned_rows():
+    lib = load_library()
+    lib.cavity_last_error.restype = ct.c_char_p
+    S, il, r, phi = random_operands(6, 6, 5, seed=3)
+    with pytest.raises(RuntimeError, match='multiple of 4'):
+        call_fdm(lib, 'cavity_fdm_pass_tf32', S, il, r, phi)
