@@ -155,6 +155,11 @@ def profile_traffic(workload):
     return None
 
 
+def sweep_kernel_name():
+    """The momentum-sweep kernel the library runs: the shared-memory tile kernel unless CAVITY_SWEEP=face."""
+    return 'momentum_kernel' if os.environ.get('CAVITY_SWEEP') == 'face' else 'sweep_tile_kernel'
+
+
 def momentum_bytes(settings, field_bytes):
     """Algorithmic HBM bytes of one momentum-sweep launch: per component 4 face arrays (read u, m and the RK
     base or write it, write the new impulse), each element once."""
@@ -264,14 +269,14 @@ def run_ours(args, ranks):
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64' if precision == 'fp64' else 'f32',
         'data': 'synthetic (seeded Gaussian initial noise, numpy default_rng)',
         'config': {'workload': args.workload, 'grid': [s['nx'], s['ny'], s['nz']], 'precision': precision,
-                   'stretch_beta': 1.5 if s.get('grid_stretch') else None, 're': round(1.0 / s['nu']),
+                   'stretch_beta': w.get('beta'), 're': round(1.0 / s['nu']),
                    'l2': 'flushed before each timed step (256 MiB write)', 'parallelism': f'replicas x{ranks.world}',
                    'device_bytes': device_bytes},
         'e2e': {'value': ranks.world * cells * args.steps / e2e_s, 'unit': 'cell-updates/s',
                 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
         'gpu_launches': launches,
         'pressure_passes_per_stage': passes / (3 * (args.steps + args.warmup)) if args.steps else None,
-        'roofline': {'kernel': 'momentum_kernel', 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+        'roofline': {'kernel': sweep_kernel_name(), 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                      'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': profile_traffic(args.workload), 'ms_per_launch': kernel_s * 1e3},
         'clocks': clocks.summary(),

@@ -48,14 +48,14 @@ def settings(n, re, nz=None, beta=None, lid='regularised', adaptive=True, cfl=0.
 # C1: plain FP64, 32^3 uniform, Re 400, polynomial lid, fixed dt 2e-3, 500 steps, noise 1e-4, 4 probes
 C1 = dict(name='c1_32cube_re400', settings=settings(32, 400.0, lid='polynomial', adaptive=False, dt_fixed=2e-3,
                                                     probes=PROBES4),
-          steps=500, noise=1e-4, seed=0, kicks=(), stats_from=None)
+          steps=500, noise=1e-4, seed=0, kicks=(), stats_from=None, beta=None)
 # C2: plain FP64 at the repo's size, 64^3 stretched (beta 1.5), Re 1000, regularised lid, CFL 0.5, 2000 steps,
 # noise 1e-3, kicks 1e-2 at steps 500 and 1000, mid-span statistics from step 1000, 8 probes
 C2 = dict(name='c2_64cube_re1000', settings=settings(64, 1000.0, beta=1.5, cfl=0.5), steps=2000, noise=1e-3, seed=0,
-          kicks=((500, 1e-2), (1000, 1e-2)), stats_from=1000)
+          kicks=((500, 1e-2), (1000, 1e-2)), stats_from=1000, beta=1.5)
 # C3: mixed precision, 128^3 stretched (beta 2.0), Re 3200, CFL 0.5, 1000 steps, noise 1e-3
 C3 = dict(name='c3_128cube_re3200', settings=settings(128, 3200.0, beta=2.0, cfl=0.5), steps=1000, noise=1e-3,
-          seed=0, kicks=(), stats_from=None, precision='mixed')
+          seed=0, kicks=(), stats_from=None, precision='mixed', beta=2.0)
 
 WORKLOADS = {w['name']: w for w in (C1, C2, C3)}
 
