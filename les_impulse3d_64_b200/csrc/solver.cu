@@ -112,10 +112,14 @@ public:
         check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
         setup_params();
         {
-            // mixed form: FDM transforms on the tcgen05 tensor cores (3xTF32) unless CAVITY_FDM=dmma; their float4
-            // row loads need nx % 4 == 0, otherwise the FP64 DMMA transforms run
+            // Mixed form: FDM transforms on the tcgen05 tensor cores (3xTF32) from 128^3 cells up, FP64 DMMA
+            // transforms below.  FP32 transforms need two refinement passes where FP64 ones need one, which
+            // only pays once the transforms are large; CAVITY_FDM=tc or =dmma forces either.  The tensor-core
+            // kernel's float4 row loads need nx % 4 == 0.
             const char* f = std::getenv("CAVITY_FDM");
-            tc_fdm_ = sizeof(T) == 4 && nx_ % 4 == 0 && !(f && std::string(f) == "dmma");
+            const std::string fdm = f ? f : "";
+            const bool want = fdm == "tc" || (fdm != "dmma" && n_cell_ >= (1LL << 21));
+            tc_fdm_ = sizeof(T) == 4 && nx_ % 4 == 0 && want;
         }
         allocate();
         upload_tables();
@@ -472,6 +476,10 @@ private:
                         zero ? 0.0 : 1.0 / (e[2].lambda[z] + e[1].lambda[y] + e[0].lambda[x]);
                 }
         check(cudaMemcpy(inv_lambda_, inv.data(), sizeof(double) * n_cell_, cudaMemcpyHostToDevice));
+        // The arena's zero-fills and these uploads run on the legacy default stream, and a copy from pageable
+        // memory may return before its DMA has landed; stream_ is non-blocking, so wait for all of it before
+        // kernels on stream_ read the uploaded operators.
+        check(cudaDeviceSynchronize());
         if (tc_fdm_) {
             // float S and 1/lambda as the reference keeps them (backend.cu:766-786), S split into hi/lo TF32
             // images of its rows (img 0, 1) and of its columns = rows of S^T (img 2, 3)
@@ -491,6 +499,7 @@ private:
         fdm_.inv_lambda = inv_lambda_;
         const std::vector<int> cells = probe_cells(c_, ax_);
         if (!cells.empty()) check(cudaMemcpy(probe_cells_, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+        check(cudaDeviceSynchronize());
         push_control();
     }
 

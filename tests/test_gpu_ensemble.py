@@ -27,3 +27,17 @@ def test_ensemble_matches_alone():
             alone.close()
         for k in f:
             assert np.array_equal(f[k], together[i][k]), (i, k)
+
+
+def test_many_mixed_cavities_set_up_and_converge():
+    """128 mixed-form cavities created back to back, each initialised (a projection from noise) and stepped:
+    every pressure solve converges.  Creating many solvers keeps the default stream busy with set-up copies;
+    each solver's first kernels must still see its uploaded operators."""
+    cases = workloads.ensemble_cases(count=128, seed=5, sizes=(32, 48, 64))
+    ens = Ensemble(cases)
+    try:
+        reports = ens.advance(2, chunk=2)
+        for rep in reports:
+            assert rep['steps'] == 2 and rep['phi_rel'] <= 1e-9
+    finally:
+        ens.close()

@@ -44,7 +44,8 @@ def test_tensor_core_transforms_match_fp64_transforms(n, steps):
     """Mixed form, tcgen05 3xTF32 transforms vs the FP64 DMMA transforms (CAVITY_FDM=dmma): both refine the
     pressure to fdm_rtol, so the fields agree to FP32 level."""
     s = workloads.settings(n, 1000.0, beta=1.5, cfl=0.5)
-    r_tc, f_tc, d_tc = run(lambda x: Solver(x, precision='mixed'), s, steps, 1e-3, 0)
+    r_tc, f_tc, d_tc = with_env('CAVITY_FDM', 'tc', lambda: run(lambda x: Solver(x, precision='mixed'), s, steps,
+                                                                  1e-3, 0))
     r_dm, f_dm, d_dm = with_env('CAVITY_FDM', 'dmma', lambda: run(lambda x: Solver(x, precision='mixed'), s, steps,
                                                                     1e-3, 0))
     for a, b in zip(r_tc, r_dm):
@@ -55,12 +56,14 @@ def test_tensor_core_transforms_match_fp64_transforms(n, steps):
     assert d_tc['div_rms'] <= 1e-5
 
 
+@pytest.mark.parametrize('fdm', ['tc', 'dmma'])
 @pytest.mark.parametrize('workload, steps', [('c1_32cube_re400', 100), ('c2_64cube_re1000', 30)])
-def test_mixed_matches_fp64_oracle(oracle_libs, workload, steps):
-    """Mixed form vs the FP64 oracle on the same seeded run: velocity within 1e-5 relative L2; the divergence
-    invariant of the reference's own check (div_rms < 1e-5)."""
+def test_mixed_matches_fp64_oracle(oracle_libs, workload, steps, fdm):
+    """Mixed form, with either transform path, vs the FP64 oracle on the same seeded run: velocity within 1e-5
+    relative L2; the divergence invariant of the reference's own check (div_rms < 1e-5)."""
     w = workloads.WORKLOADS[workload]
-    r_gpu, f_gpu, d_gpu = run(lambda x: Solver(x, precision='mixed'), w['settings'], steps, w['noise'], w['seed'])
+    r_gpu, f_gpu, d_gpu = with_env('CAVITY_FDM', fdm, lambda: run(lambda x: Solver(x, precision='mixed'),
+                                                                   w['settings'], steps, w['noise'], w['seed']))
     r_orc, f_orc, _ = run(lambda x: Solver(x, library=oracle_libs['fp64']), w['settings'], steps, w['noise'],
                           w['seed'])
     assert [r['dt_reason'] for r in r_gpu] == [r['dt_reason'] for r in r_orc]

@@ -28,6 +28,16 @@ def test_mixed_matches_reference_fixture(name):
     assert compare(out, ref, field_rtol=2e-5, passes='any', div_atol=1e-5) == []
 
 
+@pytest.mark.parametrize('name', sorted(CASES))
+def test_mixed_tensor_core_transforms_match_reference_fixture(name, monkeypatch):
+    """The mixed form with its FDM transforms forced onto the tcgen05 tensor cores (the default below 128^3
+    cells is the FP64 DMMA transforms)."""
+    monkeypatch.setenv('CAVITY_FDM', 'tc')
+    ref = dict(np.load(GOLDEN / f'{name}.npz'))
+    out = run_case(lambda s: Solver(s, precision='mixed'), CASES[name])
+    assert compare(out, ref, field_rtol=2e-5, passes='any', div_atol=1e-5) == []
+
+
 def _run_steps(make, case_settings, steps, noise, seed):
     sim = make(case_settings)
     try:
