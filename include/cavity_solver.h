@@ -97,6 +97,18 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 CavitySolver* cavity_default(void);
 /* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */
 int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
+/* Batches (no counterpart in the reference): cavities of the same grid size and precision form stepped
+ * together by one CUDA graph per step, each of whose kernel launches covers every cavity.  Every cavity keeps
+ * its own dt, pass count, clock and errors, and stays usable through its own handle between steps.  The
+ * members must have no queued steps when the batch is created; destroy the batch before its members.
+ * cavity_batch_sync waits for the queued steps and fills `reports` (one per member, in order); if a member's
+ * step failed it reports that member's last good state and returns 1 with the error, naming the member.  A
+ * batch whose members' states have diverged (a failed step) refuses further steps. */
+typedef struct CavityBatch CavityBatch;
+int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** out);
+int cavity_batch_step_async(CavityBatch* b, int count);
+int cavity_batch_sync(CavityBatch* b, CavityReport* reports);
+int cavity_batch_destroy(CavityBatch* b);
 /* One pass of the fast-diagonalisation pressure solve on caller-provided device arrays (the operation of
  * backend.cu:801-814 without the rms scaling): phi += S_x S_y S_z (inv_lambda .* (S_z^T S_y^T S_x^T r)), each
  * S applied along its axis.  s[a] / st[a]: the row-major n_a x n_a eigenbasis of axis a (eigenvector j in

@@ -295,6 +295,43 @@ class Cavity:
             self.handle = ct.c_void_p()
 
 
+class Batch:
+    """Cavities of the same grid size and form stepped together (cavity_batch_* functions): every kernel launch
+    of a batched step covers all of them.  The cavities stay ordinary `Cavity` handles between steps (fields,
+    probes, diagnostics); close the batch before closing them."""
+
+    def __init__(self, cavities):
+        if not cavities:
+            raise ValueError('a batch needs at least one cavity')
+        self.cavities = list(cavities)
+        self.lib = L = self.cavities[0].lib
+        L.cavity_batch_create.argtypes = [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_void_p)]
+        L.cavity_batch_step_async.argtypes = [ct.c_void_p, ct.c_int]
+        L.cavity_batch_sync.argtypes = [ct.c_void_p, ct.c_void_p]
+        L.cavity_batch_destroy.argtypes = [ct.c_void_p]
+        handles = (ct.c_void_p * len(self.cavities))(*[c.handle.value for c in self.cavities])
+        self.handle = ct.c_void_p()
+        self._call('cavity_batch_create', handles, len(self.cavities), ct.byref(self.handle))
+
+    def _call(self, name, *args):
+        if getattr(self.lib, name)(*args):
+            raise RuntimeError(self.lib.cavity_last_error().decode())
+
+    def step_async(self, count=1):
+        self._call('cavity_batch_step_async', self.handle, int(count))
+
+    def sync(self):
+        """Wait for the queued steps; the report of every cavity."""
+        reports = (Report * len(self.cavities))()
+        self._call('cavity_batch_sync', self.handle, reports)
+        return [Solver._as_dict(r) for r in reports]
+
+    def close(self):
+        if self.handle:
+            self._call('cavity_batch_destroy', self.handle)
+            self.handle = ct.c_void_p()
+
+
 def estimate_bytes(settings, precision='fp64', library=None):
     """Device bytes a cavity with these settings would hold (for admission against a memory budget)."""
     lib = load_library(library)

@@ -38,23 +38,22 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // CTA tile BM x BN from WARPS_M x WARPS_N warps; K consumed in panels of KC with every load of a panel in
 // flight at once (cp.async, zero-filled outside the matrices).
 template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
-__global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_kernel(GemmArgs<double> g) {
+__device__ void dgemm_mma_body(const GemmArgs<double>& g, const Blk& blk, bool first) {
     constexpr int NT = WARPS_M * WARPS_N * 32;
     constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;     // warp tile
     constexpr int FM = WTM / 8, FN = WTN / 8;                   // fragments per warp tile
     constexpr int LDA = KC + 4, LDB = BN + 4;                   // row pitches of 8 banks mod 32
     __shared__ double As[BM * LDA];
     __shared__ double Bs[KC * LDB];
-    if (g.clear_condition && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
-        cudaGraphSetConditional(g.handle, 0u);
+    if (g.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(g.handle, 0u);
     const Control* c = g.c;
-    if (c->error) return;
+    if (c->error || !c->cond) return;                     // failed, or this cavity's refinement has ended
     const double r2 = c->use_rhs ? c->rhs_norm2 : c->res_norm2;       // a zero residual: no pass (backend.cu:803-804)
     if (!(r2 > 0)) return;
-    const int b = blockIdx.z;
+    const int b = blk.z;
     const double* A = (g.A_alt && c->use_rhs ? g.A_alt : g.A) + b * g.sA;
     const double* B = g.B + b * g.sB;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int m0 = blk.y * BM, n0 = blk.x * BN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = warp / WARPS_N, wn = warp % WARPS_N;
     const int fr = lane >> 2, fc = lane & 3;          // fragment row / column of this lane
@@ -110,6 +109,21 @@ __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_kernel(GemmA
     }
 }
 
+template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
+__global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_kernel(GemmArgs<double> g) {
+    dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, real_blk(), first_block());
+}
+// a batch of cavities: grid z runs over cavities x `per` transform batches
+template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
+__global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_batched(const GemmArgs<double>* args,
+                                                                            unsigned int per) {
+    __shared__ GemmArgs<double> g;
+    int cav;
+    const Blk k = batch_blk(per, cav);
+    load_args(g, args + cav);
+    dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, k, first_block());
+}
+
 // one batched transform launch; the tile shape keeps at least ~two CTAs per SM on small grids
 inline void launch_transform(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda,
                              long long sA, const double* B, int ldb, long long sB, double* C, int ldc, long long sC,
@@ -128,10 +142,10 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
     const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch;
     if (tiles64 >= 296) {
         dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
-        dgemm_mma_kernel<64, 64, 2, 2, 32><<<grid, 128, 0, st>>>(g);
+        if (!record_launch(kLkDgemm64, 0, grid, 0, g)) dgemm_mma_kernel<64, 64, 2, 2, 32><<<grid, 128, 0, st>>>(g);
     } else {
         dim3 grid((N + 31) / 32, (M + 31) / 32, batch);
-        dgemm_mma_kernel<32, 32, 2, 2, 64><<<grid, 128, 0, st>>>(g);
+        if (!record_launch(kLkDgemm32, 0, grid, 0, g)) dgemm_mma_kernel<32, 32, 2, 2, 64><<<grid, 128, 0, st>>>(g);
     }
 }
 
@@ -162,6 +176,7 @@ inline Control standalone_fdm_control() {
     memset(&c, 0, sizeof c);
     c.res_norm2 = 1.0;
     c.rhs_norm2 = 1.0;
+    c.cond = 1;
     return c;
 }
 

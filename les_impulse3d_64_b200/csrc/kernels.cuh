@@ -18,9 +18,31 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "layout.h"
 
 namespace cavity {
+
+// ------------------------------------------------------------------------------------------ launch recording
+// Host side.  While a recorder is installed on the calling thread, the launch helpers of a solver append their
+// launch (kind, template variant, grid, dynamic shared memory and argument record) to it instead of launching:
+// a batch of cavities collects every member's arguments for the same launch sequence this way and issues one
+// batched launch per entry.
+enum LaunchKind : int { kLkStepBegin = 0, kLkSweep, kLkStart, kLkResidual, kLkFinish, kLkDgemm64, kLkDgemm32, kLkTc };
+struct LaunchRecord {
+    int kind, variant;
+    dim3 grid;
+    size_t smem;
+    std::vector<unsigned char> args;
+};
+inline thread_local std::vector<LaunchRecord>* g_launch_record = nullptr;
+template <class A> inline bool record_launch(int kind, int variant, dim3 grid, size_t smem, const A& a) {
+    if (!g_launch_record) return false;
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&a);
+    g_launch_record->push_back(LaunchRecord{kind, variant, grid, smem, std::vector<unsigned char>(b, b + sizeof a)});
+    return true;
+}
 
 constexpr int kThreads = 256;
 constexpr int X = 0, Y = 1, Z = 2;
@@ -138,13 +160,35 @@ __device__ Vec<N> block_reduce(Vec<N> x) {
     return x;   // valid in thread 0
 }
 
+// ------------------------------------------------------------------------------------------ batches
+// A kernel body sees its block index and grid through a Blk: the launch's own (real_blk) when it runs for one
+// cavity, or its cavity's share of a batched launch (batch_blk), where the cavities of a batch follow each other
+// along grid axis z, `per` z-blocks each, and every block reads its cavity's arguments from a device array.
+struct Blk {
+    unsigned int x, y, z, nx, ny, nz;
+};
+__device__ __forceinline__ Blk real_blk() { return {blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z}; }
+__device__ __forceinline__ Blk batch_blk(unsigned int per, int& cavity) {
+    cavity = (int)(blockIdx.z / per);
+    return {blockIdx.x, blockIdx.y, blockIdx.z % per, gridDim.x, gridDim.y, per};
+}
+__device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0; }
+// copy a cavity's kernel arguments into shared memory (the whole block, then a barrier)
+template <class A> __device__ __forceinline__ void load_args(A& dst, const A* src) {
+    static_assert(sizeof(A) % 4 == 0, "argument records are copied in words");
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(A) / 4); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
 // Write this block's partials; returns true in every thread of the last block to finish, after which the
 // partials of all blocks are visible to it.  The last block resets the counter for the next launch.
 template <int N>
-__device__ bool publish_partials(const Vec<N>& blk, double* partial, unsigned int* counter) {
+__device__ bool publish_partials(const Vec<N>& blk, double* partial, unsigned int* counter, const Blk& k) {
     __shared__ bool last;
-    const unsigned int nblocks = gridDim.x * gridDim.y;
-    const unsigned int b = blockIdx.x + gridDim.x * blockIdx.y;
+    const unsigned int nblocks = k.nx * k.ny;
+    const unsigned int b = k.x + k.nx * k.y;
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < N; k++) partial[k * nblocks + b] = blk.v[k];
@@ -157,10 +201,15 @@ __device__ bool publish_partials(const Vec<N>& blk, double* partial, unsigned in
     return last;
 }
 
+template <int N>
+__device__ bool publish_partials(const Vec<N>& blk, double* partial, unsigned int* counter) {
+    return publish_partials(blk, partial, counter, real_blk());
+}
+
 // In the last block: reduce all partials in a fixed order.  Result valid in thread 0.
 template <int N, bool MAX>
-__device__ Vec<N> final_reduce(const double* partial) {
-    const unsigned int nblocks = gridDim.x * gridDim.y;
+__device__ Vec<N> final_reduce(const double* partial, const Blk& k) {
+    const unsigned int nblocks = k.nx * k.ny;
     Vec<N> acc;
 #pragma unroll
     for (int k = 0; k < N; k++) {
@@ -171,11 +220,19 @@ __device__ Vec<N> final_reduce(const double* partial) {
     }
     return block_reduce<N, MAX>(acc);
 }
+template <int N, bool MAX>
+__device__ Vec<N> final_reduce(const double* partial) {
+    return final_reduce<N, MAX>(partial, real_blk());
+}
 
 // ------------------------------------------------------------------------------------------ step begin
 // dt from the CFL rate of the current velocity and the viscous rate (backend.cu:884-899).
-__global__ void step_begin_kernel(Params p, Control* c) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+struct StepBeginArgs {
+    Params p;
+    Control* c;
+};
+__device__ void step_begin_body(const Params& p, Control* c) {
+    if (threadIdx.x != 0) return;
     if (c->error) return;          // an earlier queued step failed: leave everything as it is
     const double rates[2] = {(double)(float)c->cfl_rate, p.viscous_rate};
     double use[2] = {rates[0], rates[1]};
@@ -197,6 +254,14 @@ __global__ void step_begin_kernel(Params p, Control* c) {
     if (p.dt_lag && c->last_dt > 0) dt = fmin(dt, 1.1 * c->last_dt);
     c->dt = dt;
     c->use0 = use[0];
+}
+__global__ void step_begin_kernel(Params p, Control* c) {
+    if (blockIdx.x == 0) step_begin_body(p, c);
+}
+// one block per cavity of the batch
+__global__ void step_begin_batched(const StepBeginArgs* args) {
+    const StepBeginArgs& a = args[blockIdx.z];
+    step_begin_body(a.p, a.c);
 }
 
 // ------------------------------------------------------------------------------------------ stage constants
@@ -289,9 +354,12 @@ __device__ __forceinline__ void guess_coefficients(const Params& p, const Contro
     }
 }
 
+// use_handle: 0 = no graph loop, 1 = this cavity's own loop, 2 = a loop shared by a batch of cavities, which
+// runs while any cavity needs it (only ever set here; the first transform of each pass clears it)
 __device__ __forceinline__ void set_loop(Control* c, cudaGraphConditionalHandle h, int use_handle, int cond) {
     c->cond = cond;
-    if (use_handle) cudaGraphSetConditional(h, cond ? 1u : 0u);
+    if (use_handle == 1) cudaGraphSetConditional(h, cond ? 1u : 0u);
+    else if (use_handle == 2 && cond) cudaGraphSetConditional(h, 1u);
 }
 
 // decision after a residual: more passes, convergence, or the non-convergence error (backend.cu:832-845)
@@ -307,7 +375,7 @@ __device__ __forceinline__ void decide_loop(const Params& p, Control* c, cudaGra
 }
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T> a) {
+__device__ void projection_start_body(const StartArgs<T>& a, const Blk& k) {
     Control* c = a.c;
     const Params& p = a.p;
     const int err = c->error;
@@ -330,7 +398,7 @@ __global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T>
     acc.v[0] = acc.v[1] = acc.v[2] = 0.0;
     const int sy = p.nx, sz = p.nx * p.ny;
     if (!err) {
-        for (int i = blockIdx.x * kThreads + threadIdx.x; i < p.n_cell; i += gridDim.x * kThreads) {
+        for (int i = k.x * kThreads + threadIdx.x; i < p.n_cell; i += k.nx * kThreads) {
             const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
             const double dx = a.g.dw[X][x], dy = a.g.dw[Y][y], dz = a.g.dw[Z][z];
             const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
@@ -361,8 +429,8 @@ __global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T>
         }
     }
     const Vec<3> blk = block_reduce<3, false>(acc);
-    if (publish_partials(blk, a.partial, &c->counter[kCntDiv])) {
-        const Vec<3> tot = final_reduce<3, false>(a.partial);
+    if (publish_partials(blk, a.partial, &c->counter[kCntDiv], k)) {
+        const Vec<3> tot = final_reduce<3, false>(a.partial, k);
         if (threadIdx.x == 0) {
             c->counter[kCntDiv] = 0;
             c->passes = 0;
@@ -397,6 +465,18 @@ __global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T>
         }
     }
 }
+template <class T>
+__global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T> a) {
+    projection_start_body(a, real_blk());
+}
+template <class T>
+__global__ void __launch_bounds__(kThreads) projection_start_batched(const StartArgs<T>* args) {
+    __shared__ StartArgs<T> a;
+    int cav;
+    const Blk k = batch_blk(1, cav);
+    load_args(a, args + cav);
+    projection_start_body(a, k);
+}
 
 // ------------------------------------------------------------------------------------------ residual
 // r = rhs - L phi with L the 7-point area-weighted Neumann Laplacian (backend.cu:345-359) after a pass, sum r^2
@@ -414,8 +494,10 @@ struct ResidualArgs {
     int use_handle;
 };
 
-__global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) {
+// A cavity whose refinement loop has ended (a batch runs passes while any cavity needs one) skips the pass.
+__device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     Control* c = a.c;
+    if (!c->cond) return;
     const Params& p = a.p;
     const int err = c->error;
     Vec<2> acc;
@@ -423,7 +505,7 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) {
     acc.v[1] = 0.0;
     const int sy = p.nx, sz = p.nx * p.ny;
     if (!err) {
-        for (int i = blockIdx.x * kThreads + threadIdx.x; i < p.n_cell; i += gridDim.x * kThreads) {
+        for (int i = k.x * kThreads + threadIdx.x; i < p.n_cell; i += k.nx * kThreads) {
             const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
             const double dx = a.dw[X][x], dy = a.dw[Y][y], dz = a.dw[Z][z];
             const double* f = a.phi;
@@ -442,8 +524,8 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) {
         }
     }
     const Vec<2> blk = block_reduce<2, false>(acc);
-    if (publish_partials(blk, a.partial, &c->counter[kCntRes])) {
-        const Vec<2> tot = final_reduce<2, false>(a.partial);
+    if (publish_partials(blk, a.partial, &c->counter[kCntRes], k)) {
+        const Vec<2> tot = final_reduce<2, false>(a.partial, k);
         if (threadIdx.x == 0) {
             c->counter[kCntRes] = 0;
             if (err) { set_loop(c, a.handle, a.use_handle, 0); return; }
@@ -459,6 +541,14 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) {
             decide_loop(p, c, a.handle, a.use_handle);
         }
     }
+}
+__global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
+__global__ void __launch_bounds__(kThreads) residual_batched(const ResidualArgs* args) {
+    __shared__ ResidualArgs a;
+    int cav;
+    const Blk k = batch_blk(1, cav);
+    load_args(a, args + cav);
+    residual_body(a, k);
 }
 
 // ------------------------------------------------------------------------------------------ FDM transforms
@@ -508,7 +598,7 @@ template <class T> struct FinishArgs {
 };
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
+__device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
     Control* c = a.c;
     const Params& p = a.p;
     const int err = c->error;
@@ -527,7 +617,7 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
     const double mean = c->phi_sum / p.n_cell;
     const int sy = p.nx, sz = p.nx * p.ny;
     auto pv = [&](int j) { return zero_phi ? 0.0 : a.phi[j] - mean; };
-    for (int i = err ? p.n_cell : blockIdx.x * kThreads + threadIdx.x; i < p.n_cell; i += gridDim.x * kThreads) {
+    for (int i = err ? p.n_cell : k.x * kThreads + threadIdx.x; i < p.n_cell; i += k.nx * kThreads) {
         const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
         const double ph = pv(i);
         // faces below this cell (wall faces 0), and above it at the last cell of an axis
@@ -557,8 +647,8 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
     }
     // gridwide: CFL max (NaN wins) and the scalar bookkeeping in the last block
     const Vec<1> blk = block_reduce<1, true>(acc);
-    if (publish_partials(blk, a.partial, &c->counter[kCntFinish])) {
-        const Vec<1> tot = final_reduce<1, true>(a.partial);
+    if (publish_partials(blk, a.partial, &c->counter[kCntFinish], k)) {
+        const Vec<1> tot = final_reduce<1, true>(a.partial, k);
         if (threadIdx.x == 0) {
             c->counter[kCntFinish] = 0;
             if (!err) {
@@ -588,6 +678,16 @@ __global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) {
             }
         }
     }
+}
+template <class T>
+__global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) { finish_body(a, real_blk()); }
+template <class T>
+__global__ void __launch_bounds__(kThreads) finish_batched(const FinishArgs<T>* args) {
+    __shared__ FinishArgs<T> a;
+    int cav;
+    const Blk k = batch_blk(1, cav);
+    load_args(a, args + cav);
+    finish_body(a, k);
 }
 
 // ------------------------------------------------------------------------------------------ small kernels

@@ -91,7 +91,10 @@ public:
 };
 
 // ------------------------------------------------------------------------------------------ the solver
+template <class T> class Batch;
+
 template <class T> class Solver : public SolverBase {
+    friend class Batch<T>;
     // tile of the shared-memory sweep: 32 x TY x TZ cells (about 113 KB of shared memory in FP64, 85 KB in FP32)
     static constexpr int kTileTY = sizeof(T) == 8 ? 4 : 8;
     static constexpr int kTileTZ = 4;
@@ -556,6 +559,12 @@ private:
     }
 
     // ------------------------------------------------------------------------------ kernel launches
+    void launch_step_begin(cudaStream_t st) {
+        StepBeginArgs a;
+        a.p = p_;
+        a.c = ctrl_;
+        if (!record_launch(kLkStepBegin, 0, dim3(1), 0, a)) step_begin_kernel<<<1, 32, 0, st>>>(p_, ctrl_);
+    }
     void launch_momentum(cudaStream_t st, int stage, int S, int in, int out) {
         MomentumArgs<T> a;
         a.p = p_;
@@ -575,15 +584,17 @@ private:
         if (tile_sweep_) {
             using G = TileGeom<kTileTY, kTileTZ>;
             dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
-            sweep_tile_kernel<T, kTileTY, kTileTZ><<<grid, kTileThreads, G::template smem_bytes<T>(), st>>>(a);
+            if (!record_launch(kLkSweep, 0, grid, G::template smem_bytes<T>(), a))
+                sweep_tile_kernel<T, kTileTY, kTileTZ><<<grid, kTileThreads, G::template smem_bytes<T>(), st>>>(a);
         } else {
             dim3 grid(blocks_for(max_face_), 3);
             momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
         }
     }
     // rhs, starting potential and its residual, start-of-solve decisions (backend.cu:816-831)
+    // use_h: 0 no graph loop, 1 this solver's own loop, 2 a loop shared by a batch (see set_loop)
     void launch_start(cudaStream_t st, T* const m[3], bool step_mode, int stage, int S, int cur,
-                      cudaGraphConditionalHandle h, bool use_h) {
+                      cudaGraphConditionalHandle h, int use_h) {
         StartArgs<T> a;
         a.p = p_;
         a.g = geo_;
@@ -601,9 +612,9 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        projection_start_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkStart, 0, dim3(cell_blocks_), 0, a)) projection_start_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
     }
-    void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, bool use_h) {
+    void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, int use_h) {
         ResidualArgs a;
         a.p = p_;
         for (int k = 0; k < 3; k++) { a.dw[k] = geo_.dw[k]; a.dinv_sp[k] = geo_.dinv_sp[k]; }
@@ -614,12 +625,12 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        residual_kernel<<<cell_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkResidual, 0, dim3(cell_blocks_), 0, a)) residual_kernel<<<cell_blocks_, kThreads, 0, st>>>(a);
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
-    void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
-        if (tc_fdm_) launch_tc_pass(st, phi, h, use_h);
-        else launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h);
+    void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
+        if (tc_fdm_) launch_tc_pass(st, phi, h, use_h != 0);
+        else launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h != 0);
         launch_residual(st, phi, h, use_h);
     }
     void launch_tc_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
@@ -641,7 +652,7 @@ private:
         a.stage = stage;
         a.c = ctrl_;
         a.partial = partial_;
-        finish_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkFinish, 0, dim3(cell_blocks_), 0, a)) finish_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
     }
 
     // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
@@ -666,7 +677,7 @@ private:
         check(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         check(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        launch_pass(body_stream_, phi, h, true);
+        launch_pass(body_stream_, phi, h, 1);
         check(cudaStreamEndCapture(body_stream_, &body));
         check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
     }
@@ -680,7 +691,7 @@ private:
             if (eager) check(cudaEventRecord(e, stream_));
             else check(cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal));
         };
-        step_begin_kernel<<<1, 32, 0, stream_>>>(p_, ctrl_);
+        launch_step_begin(stream_);
         for (int stage = 0; stage < 3; stage++) {
             const int in = stage == 0 ? S : stage == 1 ? Xs : Ys;
             const int out = stage == 1 ? Ys : Xs;
@@ -690,14 +701,14 @@ private:
             if (timing) mark(kev_[2 * stage + 1]);
             double* phi = praw_;          // the solve works here; finish writes PHI_[out]
             if (eager) {
-                launch_start(stream_, M_[out], true, stage, S, cur, 0, false);
+                launch_start(stream_, M_[out], true, stage, S, cur, 0, 0);
                 pull_control();
                 while (hc_.cond && !hc_.error) {
-                    launch_pass(stream_, phi, 0, false);
+                    launch_pass(stream_, phi, 0, 0);
                     pull_control();
                 }
             } else {
-                captured_loop([&](cudaGraphConditionalHandle h) { launch_start(stream_, M_[out], true, stage, S, cur, h, true); },
+                captured_loop([&](cudaGraphConditionalHandle h) { launch_start(stream_, M_[out], true, stage, S, cur, h, 1); },
                               phi);
             }
             launch_finish(stream_, M_[out], U_[out], PHI_[out], true, stage, stage == 2);
@@ -736,11 +747,11 @@ private:
         hc_.error = kOk;
         push_control();
         for (int k = 0; k < 3; k++) zero_walls_kernel<T><<<blocks_for(size_[k]), kThreads, 0, stream_>>>(p_, k, m[k]);
-        launch_start(stream_, m, false, 0, par_, par_, 0, false);
+        launch_start(stream_, m, false, 0, par_, par_, 0, 0);
         pull_control();
         int guard = 0;
         while (hc_.cond && !hc_.error && guard++ < 1000) {
-            launch_pass(stream_, praw_, 0, false);
+            launch_pass(stream_, praw_, 0, 0);
             pull_control();
         }
         if (hc_.error) {
@@ -795,6 +806,194 @@ private:
     cudaGraphExec_t exec_[2] = {nullptr, nullptr}, texec_[2] = {nullptr, nullptr};
     cudaEvent_t kev_[6] = {};
     void* flush_ = nullptr;
+};
+
+
+// ------------------------------------------------------------------------------------------------ batches
+// B cavities of the same grid size and form stepped together by one CUDA graph per state parity, each of whose
+// kernel launches covers every cavity (the batched entries of the kernels: grid axis z runs over the cavities,
+// and each block reads its cavity's argument record from a device array).  The launch sequence and the
+// argument records are the members' own: each member's launch helpers run with a recorder installed.  The
+// refinement loop of a stage runs while any cavity needs another pass; a cavity whose solve has ended skips
+// the later passes.  Every cavity keeps its own control block, dt, pass count, clock and errors, and stays a
+// full solver between steps (getters, kick, fields through its own handle).
+class BatchBase {
+public:
+    virtual ~BatchBase() {}
+    virtual void step_async(int count) = 0;
+    virtual void sync(CavityReport* reports) = 0;
+    virtual int size() const = 0;
+};
+
+template <class T> class Batch : public BatchBase {
+    using S_ = Solver<T>;
+    static constexpr int kTY = S_::kTileTY, kTZ = S_::kTileTZ;
+
+public:
+    explicit Batch(const std::vector<S_*>& members) : m_(members) {
+        if (m_.empty()) fail("batch: no cavities");
+        const S_& f = *m_[0];
+        for (const S_* s : m_) {
+            if (s->nx_ != f.nx_ || s->ny_ != f.ny_ || s->nz_ != f.nz_) fail("batch: every cavity needs the same grid size");
+            if (s->tc_fdm_ != f.tc_fdm_ || !s->tile_sweep_) fail("batch: every cavity needs the same kernels (tile sweep)");
+            if (s->eager_) fail("batch: not available with CAVITY_GRAPHS=0");
+            if (!s->pending_.empty()) fail("batch: a cavity has queued steps; sync it first");
+        }
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
+        using G = TileGeom<kTY, kTZ>;
+        check(cudaFuncSetAttribute(sweep_tile_batched<T, kTY, kTZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)G::template smem_bytes<T>()));
+        if (f.tc_fdm_) check(tc_transform_prepare_batched());
+        for (int S = 0; S < 2; S++) build(S);
+    }
+    ~Batch() override {
+        if (stream_) cudaStreamSynchronize(stream_);
+        for (int S = 0; S < 2; S++) {
+            if (exec_[S]) cudaGraphExecDestroy(exec_[S]);
+            if (graph_[S]) cudaGraphDestroy(graph_[S]);
+            if (dargs_[S]) cudaFree(dargs_[S]);
+        }
+        if (stream_) cudaStreamDestroy(stream_);
+        if (body_stream_) cudaStreamDestroy(body_stream_);
+    }
+    int size() const override { return (int)m_.size(); }
+
+    void step_async(int count) override {
+        for (int i = 0; i < count; i++) {
+            const int S = m_[0]->par_;
+            for (const S_* s : m_)
+                if (s->par_ != S) fail("batch: the cavities' states have diverged (a failed step); rebuild the batch");
+            check(cudaGraphLaunch(exec_[S], stream_));
+            for (S_* s : m_) {
+                if (s->pending_.empty()) s->steps_before_ = s->hc_.steps;
+                s->pending_.push_back(s->par_);
+                s->par_ ^= 1;
+            }
+        }
+    }
+    // waits for the queued steps; every cavity's report (its last good state if it failed), then the first
+    // failure as an error naming the cavity
+    void sync(CavityReport* reports) override {
+        check(cudaStreamSynchronize(stream_));
+        std::string first;
+        for (size_t i = 0; i < m_.size(); i++) {
+            try {
+                m_[i]->sync(reports ? &reports[i] : nullptr);
+            } catch (const std::exception& e) {
+                if (first.empty()) first = "cavity " + std::to_string(i) + ": " + e.what();
+                if (reports) m_[i]->report(&reports[i]);
+            }
+        }
+        if (!first.empty()) fail(first);
+    }
+
+private:
+    struct RecordGuard {
+        explicit RecordGuard(std::vector<LaunchRecord>* r) { g_launch_record = r; }
+        ~RecordGuard() { g_launch_record = nullptr; }
+    };
+    // run `fn` on every member with a recorder installed, append the argument records of each recorded launch to
+    // `host` (one contiguous array per launch) and, when `launch`, issue the batched launches on `st`
+    template <class F> void emit(cudaStream_t st, F fn, std::vector<unsigned char>& host, bool launch) {
+        const size_t B = m_.size();
+        std::vector<std::vector<LaunchRecord>> recs(B);
+        for (size_t b = 0; b < B; b++) {
+            RecordGuard guard(&recs[b]);
+            fn(*m_[b]);
+        }
+        for (size_t b = 1; b < B; b++) {
+            bool same = recs[b].size() == recs[0].size();
+            for (size_t j = 0; same && j < recs[0].size(); j++) {
+                const LaunchRecord &x = recs[0][j], &y = recs[b][j];
+                same = x.kind == y.kind && x.variant == y.variant && x.grid.x == y.grid.x && x.grid.y == y.grid.y &&
+                       x.grid.z == y.grid.z && x.smem == y.smem && x.args.size() == y.args.size();
+            }
+            if (!same) fail("batch: the cavities' launch sequences differ");
+        }
+        for (size_t j = 0; j < recs[0].size(); j++) {
+            const size_t sz = recs[0][j].args.size();
+            const size_t off = (host.size() + 255) / 256 * 256;
+            host.resize(off + sz * B);
+            for (size_t b = 0; b < B; b++) std::memcpy(host.data() + off + b * sz, recs[b][j].args.data(), sz);
+            if (launch) launch_batched(recs[0][j], static_cast<const unsigned char*>(dargs_cur_) + off, (int)B, st);
+        }
+    }
+    void launch_batched(const LaunchRecord& r, const void* d, int B, cudaStream_t st) {
+        const dim3 g(r.grid.x, r.grid.y, r.grid.z * B);
+        const unsigned int per = r.grid.z;
+        switch (r.kind) {
+        case kLkStepBegin: step_begin_batched<<<dim3(1, 1, B), 32, 0, st>>>((const StepBeginArgs*)d); break;
+        case kLkSweep: sweep_tile_batched<T, kTY, kTZ><<<g, kTileThreads, r.smem, st>>>((const MomentumArgs<T>*)d, per); break;
+        case kLkStart: projection_start_batched<T><<<g, kThreads, 0, st>>>((const StartArgs<T>*)d); break;
+        case kLkResidual: residual_batched<<<g, kThreads, 0, st>>>((const ResidualArgs*)d); break;
+        case kLkFinish: finish_batched<T><<<g, kThreads, 0, st>>>((const FinishArgs<T>*)d); break;
+        case kLkDgemm64: dgemm_mma_batched<64, 64, 2, 2, 32><<<g, 128, 0, st>>>((const GemmArgs<double>*)d, per); break;
+        case kLkDgemm32: dgemm_mma_batched<32, 32, 2, 2, 64><<<g, 128, 0, st>>>((const GemmArgs<double>*)d, per); break;
+        case kLkTc: launch_tc_batched(r.variant, g, per, (const TcTransformArgs*)d, st); break;
+        default: fail("batch: unknown launch");
+        }
+    }
+    // the step for state parity S (as Solver::enqueue_step); `launch` = false only records (sizes the argument
+    // buffer), true captures the batched launches into the graph being built on stream_
+    void sequence(int S, std::vector<unsigned char>& host, bool launch) {
+        const int Xs = S ^ 1, Ys = 2;
+        emit(stream_, [&](S_& s) { s.launch_step_begin(stream_); }, host, launch);
+        for (int stage = 0; stage < 3; stage++) {
+            const int in = stage == 0 ? S : stage == 1 ? Xs : Ys;
+            const int out = stage == 1 ? Ys : Xs;
+            const int cur = stage == 1 ? Xs : Ys;
+            emit(stream_, [&](S_& s) { s.launch_momentum(stream_, stage, S, in, out); }, host, launch);
+            cudaGraphConditionalHandle h = 0;
+            cudaGraph_t g = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            cudaStreamCaptureStatus status;
+            if (launch) {
+                check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
+                check(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+            }
+            emit(stream_, [&](S_& s) { s.launch_start(stream_, s.M_[out], true, stage, S, cur, h, 2); }, host, launch);
+            if (launch) {
+                check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
+                cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = h;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                cudaGraphNode_t node;
+                check(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+                cudaGraph_t body = cp.conditional.phGraph_out[0];
+                check(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+                emit(body_stream_, [&](S_& s) { s.launch_pass(body_stream_, s.praw_, h, 2); }, host, launch);
+                check(cudaStreamEndCapture(body_stream_, &body));
+                check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+            } else {
+                emit(stream_, [&](S_& s) { s.launch_pass(stream_, s.praw_, h, 2); }, host, launch);
+            }
+            emit(stream_, [&](S_& s) { s.launch_finish(stream_, s.M_[out], s.U_[out], s.PHI_[out], true, stage, stage == 2); },
+                 host, launch);
+        }
+    }
+    void build(int S) {
+        std::vector<unsigned char> host;
+        sequence(S, host, false);
+        check(cudaMalloc(&dargs_[S], std::max<size_t>(host.size(), 256)));
+        dargs_cur_ = dargs_[S];
+        host.clear();
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        sequence(S, host, true);
+        check(cudaStreamEndCapture(stream_, &graph_[S]));
+        check(cudaGraphInstantiate(&exec_[S], graph_[S], 0));
+        check(cudaMemcpy(dargs_[S], host.data(), host.size(), cudaMemcpyHostToDevice));
+    }
+
+    std::vector<S_*> m_;
+    cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
+    cudaGraph_t graph_[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+    void* dargs_[2] = {nullptr, nullptr};
+    void* dargs_cur_ = nullptr;
 };
 
 static SolverBase* make_solver(const CavityConfig& c, int precision) {
@@ -966,6 +1165,7 @@ static void fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], c
 // ================================================================================================ C ABI
 using cavity::SolverBase;
 struct CavitySolver { std::unique_ptr<SolverBase> s; };
+struct CavityBatch { std::unique_ptr<cavity::BatchBase> b; };
 
 static std::string g_last_error;
 static CavitySolver* g_default = nullptr;
@@ -1074,5 +1274,35 @@ int cavity_fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], co
     return safely([&] { cavity::fdm_pass_noalloc(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
 }
 long long cavity_pressure_passes(const CavitySolver* s) { return s && s->s ? s->s->pressure_passes() : -1; }
+int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** out) {
+    return safely([&] {
+        if (!members || count < 1 || !out) cavity::fail("batch: need at least one cavity");
+        std::vector<cavity::Solver<double>*> d;
+        std::vector<cavity::Solver<float>*> f;
+        for (int i = 0; i < count; i++) {
+            SolverBase* s = &H(members[i]);
+            if (auto* p = dynamic_cast<cavity::Solver<double>*>(s)) d.push_back(p);
+            else if (auto* q = dynamic_cast<cavity::Solver<float>*>(s)) f.push_back(q);
+        }
+        if (!d.empty() && !f.empty()) cavity::fail("batch: every cavity needs the same precision form");
+        std::unique_ptr<CavityBatch> b(new CavityBatch);
+        if (!d.empty()) b->b.reset(new cavity::Batch<double>(d));
+        else b->b.reset(new cavity::Batch<float>(f));
+        *out = b.release();
+    });
+}
+int cavity_batch_step_async(CavityBatch* b, int count) {
+    return safely([&] {
+        if (!b || !b->b) cavity::fail("invalid batch handle");
+        b->b->step_async(count);
+    });
+}
+int cavity_batch_sync(CavityBatch* b, CavityReport* reports) {
+    return safely([&] {
+        if (!b || !b->b) cavity::fail("invalid batch handle");
+        b->b->sync(reports);
+    });
+}
+int cavity_batch_destroy(CavityBatch* b) { return safely([&] { delete b; }); }
 const char* cavity_last_error(void) { return g_last_error.c_str(); }
 }

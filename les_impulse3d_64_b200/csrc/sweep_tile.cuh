@@ -110,7 +110,7 @@ __device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* 
 }
 
 template <class T, int TY, int TZ>
-__global__ void __launch_bounds__(kTileThreads) sweep_tile_kernel(MomentumArgs<T> a) {
+__device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     using G = TileGeom<TY, TZ>;
     constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
     constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(kTileThreads) sweep_tile_kernel(MomentumArgs<T
     const Params& p = a.p;
     const Geo<T>& g = a.g;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    const int x0 = blk.x * TX, y0 = blk.y * TY, z0 = blk.z * TZ;
     const int o4 = p.o4;
     const bool blend = a.stage == 0;
 
@@ -340,6 +340,20 @@ __global__ void __launch_bounds__(kTileThreads) sweep_tile_kernel(MomentumArgs<T
             }
         }
     }
+}
+
+template <class T, int TY, int TZ>
+__global__ void __launch_bounds__(kTileThreads) sweep_tile_kernel(MomentumArgs<T> a) {
+    sweep_tile_body<T, TY, TZ>(a, real_blk());
+}
+// a batch of cavities: grid z runs over cavities x `per` z-tiles
+template <class T, int TY, int TZ>
+__global__ void __launch_bounds__(kTileThreads) sweep_tile_batched(const MomentumArgs<T>* args, unsigned int per) {
+    __shared__ MomentumArgs<T> a;
+    int cav;
+    const Blk k = batch_blk(per, cav);
+    load_args(a, args + cav);
+    sweep_tile_body<T, TY, TZ>(a, k);
 }
 
 }  // namespace cavity

@@ -207,22 +207,21 @@ template <int BN, int FA, int F64> struct FieldPanel {
 // grid: (N / BN tiles, M / 128 tiles, batch).  FA: the field is operand A (x transforms); F64: the field is the
 // fp64 residual, scaled by 1/rms (first transform of a pass).
 template <int BN, int FA, int F64>
-__global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArgs g) {
+__device__ void tc_transform_body(const TcTransformArgs& g, const Blk& blk, bool first) {
     using L = TcSmem<BN>;
     using P = FieldPanel<BN, FA, F64>;
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
-    if (g.clear_condition && threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
-        cudaGraphSetConditional(g.handle, 0u);
+    if (g.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(g.handle, 0u);
     // the control block is read while TMEM and the barriers are set up
     const Control* c = g.c;
-    const int err = c->error, use_rhs = c->use_rhs, reset = c->reset_phi;
+    const int err = c->error, use_rhs = c->use_rhs, reset = c->reset_phi, cond = c->cond;
     const double rhs2 = c->rhs_norm2, res2 = c->res_norm2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
-    const int b = blockIdx.z;
-    const int m0 = blockIdx.y * kTcRows, n0 = blockIdx.x * BN;
+    const int b = blk.z;
+    const int m0 = blk.y * kTcRows, n0 = blk.x * BN;
     const int row = m0 + warp * 32 + lane;
     const uint32_t sbase = smem_addr(smem);
     constexpr uint32_t kCols = BN < 32 ? 32 : BN;
@@ -238,7 +237,8 @@ __global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArg
     tc_fence_after();
     const uint32_t tmem = tmem_base;
     const double r2 = use_rhs ? rhs2 : res2;
-    if (err || !(r2 > 0)) {                                    // a zero residual: no pass (backend.cu:803-804)
+    // failed, this cavity's refinement has ended, or a zero residual: no pass (backend.cu:803-804)
+    if (err || !cond || !(r2 > 0)) {
         if (warp == 0) tmem_dealloc(tmem, kCols);
         return;
     }
@@ -429,6 +429,20 @@ __global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArg
     if (warp == 0) tmem_dealloc(tmem, kCols);
 }
 
+template <int BN, int FA, int F64>
+__global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArgs g) {
+    tc_transform_body<BN, FA, F64>(g, real_blk(), first_block());
+}
+// a batch of cavities: grid z runs over cavities x `per` transform batches
+template <int BN, int FA, int F64>
+__global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTransformArgs* args, unsigned int per) {
+    __shared__ TcTransformArgs g;
+    int cav;
+    const Blk k = batch_blk(per, cav);
+    load_args(g, args + cav);
+    tc_transform_body<BN, FA, F64>(g, k, first_block());
+}
+
 // ---------------------------------------------------------------- host side
 // tile width: the widest of 128 / 64 / 32 columns that still gives one CTA per SM, else 32
 inline int tc_pick_bn(int M, int N, int batch, int sms) {
@@ -449,6 +463,36 @@ template <int BN> inline cudaError_t tc_prepare_bn() {
                                  TcSmem<BN>::kBytes);
     return e;
 }
+template <int BN> inline cudaError_t tc_prepare_batched_bn() {
+    cudaError_t e = cudaFuncSetAttribute(tc_transform_batched<BN, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcSmem<BN>::kBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc_transform_batched<BN, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BN>::kBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc_transform_batched<BN, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcSmem<BN>::kBytes);
+    return e;
+}
+inline cudaError_t tc_transform_prepare_batched() {
+    cudaError_t e = tc_prepare_batched_bn<128>();
+    if (e == cudaSuccess) e = tc_prepare_batched_bn<64>();
+    if (e == cudaSuccess) e = tc_prepare_batched_bn<32>();
+    return e;
+}
+template <int BN>
+inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
+    if (fa && f64) tc_transform_batched<BN, 1, 1><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(d, per);
+    else if (fa) tc_transform_batched<BN, 1, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(d, per);
+    else tc_transform_batched<BN, 0, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(d, per);
+}
+// a recorded launch (variant: see tc_variant) over a batch of cavities
+inline void launch_tc_batched(int variant, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
+    const int bn = variant & 0xff, fa = (variant >> 8) & 1, f64 = (variant >> 9) & 1;
+    if (bn == 128) launch_tc_batched_bn<128>(fa, f64, grid, per, d, st);
+    else if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, per, d, st);
+    else launch_tc_batched_bn<32>(fa, f64, grid, per, d, st);
+}
 inline cudaError_t tc_transform_prepare() {
     cudaError_t e = tc_prepare_bn<128>();
     if (e == cudaSuccess) e = tc_prepare_bn<64>();
@@ -460,9 +504,14 @@ template <int BN> inline void launch_tc_bn(cudaStream_t st, const TcTransformArg
     else if (g.field_is_a) tc_transform_kernel<BN, 1, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
     else tc_transform_kernel<BN, 0, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
 }
+// variant code of a recorded launch: tile width, field-is-A, fp64 field
+inline int tc_variant(int bn, const TcTransformArgs& g) { return bn | (g.field_is_a ? 1 << 8 : 0) | (g.field64 ? 1 << 9 : 0); }
 inline void launch_tc_transform(cudaStream_t st, const TcTransformArgs& g, int batch, int sms) {
     const int bn = tc_pick_bn(g.M, g.N, batch, sms);
     const dim3 grid((g.N + bn - 1) / bn, (g.M + kTcRows - 1) / kTcRows, batch);
+    if (record_launch(kLkTc, tc_variant(bn, g), grid, (size_t)(bn == 128 ? TcSmem<128>::kBytes : bn == 64 ? TcSmem<64>::kBytes
+                                                                                                       : TcSmem<32>::kBytes), g))
+        return;
     if (bn == 128) launch_tc_bn<128>(st, g, grid);
     else if (bn == 64) launch_tc_bn<64>(st, g, grid);
     else launch_tc_bn<32>(st, g, grid);

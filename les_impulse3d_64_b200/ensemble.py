@@ -1,43 +1,65 @@
 """Many independent cavities advanced together on one GPU.
 
-Each cavity is a handle of the C ABI (`cavity_create`) with its own CUDA stream and step graphs; stepping
-enqueues graph launches on every cavity's stream before waiting for any of them, so the small, latency-bound
-kernels of different cavities run concurrently and fill the device.  Results do not depend on the mix: each
-cavity's kernels read and write only its own buffers and control block, and its reductions have a fixed order.
+Two ways of stepping them:
+
+* batched (the default): cavities of the same grid size and precision form are grouped into batches
+  (`cavity_batch_create`).  One CUDA graph steps a whole batch, and each of its kernel launches covers every
+  cavity of the batch, so a step of B cavities costs the launches of one.  Batches of different sizes run on
+  their own streams, concurrently.
+* per cavity (`batched=False`): every cavity steps through its own stream and graphs; the graph launches of all
+  cavities are enqueued before waiting for any, so small, latency-bound kernels of different cavities overlap.
+
+Results do not depend on the mix or on the way of stepping: each cavity's kernels read and write only its own
+buffers and control block, and its reductions have a fixed order.
 """
 import time
 
-import numpy as np
-
 from . import workloads
-from .api import Cavity
+from .api import Batch, Cavity
 
 
 class Ensemble:
-    def __init__(self, cases, library=None):
+    def __init__(self, cases, library=None, batched=True):
         """`cases`: dicts with `settings`, `noise`, `seed` and `precision` (see workloads.ensemble_cases)."""
         self.cases = list(cases)
         self.cavities = []
+        self.batches = []
+        self.groups = []              # member indices of each batch
         try:
             for case in self.cases:
                 cav = Cavity(case['settings'], precision=case.get('precision', 'mixed'), library=library)
                 self.cavities.append(cav)
                 cav.initialize(*workloads.initial_noise(cav.shapes, case['noise'], case['seed']))
+            if batched:
+                keys = {}
+                for i, (case, cav) in enumerate(zip(self.cases, self.cavities)):
+                    keys.setdefault((cav.nx, cav.ny, cav.nz, case.get('precision', 'mixed')), []).append(i)
+                for members in keys.values():
+                    self.batches.append(Batch([self.cavities[i] for i in members]))
+                    self.groups.append(members)
         except Exception:
             self.close()
             raise
         self.cells = [c.n_cell for c in self.cavities]
 
     def advance(self, steps, chunk=8):
-        """Advance every cavity by `steps` steps, `chunk` queued per cavity between waits; returns the reports
-        of the last step."""
+        """Advance every cavity by `steps` steps, `chunk` queued per cavity (or batch) between waits; returns the
+        reports of the last step, in case order."""
         done = 0
         reports = None
         while done < steps:
             n = min(chunk, steps - done)
-            for cav in self.cavities:
-                cav.step_async(n)
-            reports = [cav.sync() for cav in self.cavities]
+            if self.batches:
+                for b in self.batches:
+                    b.step_async(n)
+                reports = [None] * len(self.cavities)
+                for b, members in zip(self.batches, self.groups):
+                    for i, r in zip(members, b.sync()):
+                        reports[i] = r
+            else:
+                for cav in self.cavities:
+                    cav.step_async(n)
+                reports = [cav.sync() for cav in self.cavities]
             done += n
         return reports
 
@@ -56,6 +78,10 @@ class Ensemble:
         return {k: self.cavities[index].field(k) for k in names}
 
     def close(self):
+        for b in self.batches:
+            b.close()
+        self.batches = []
+        self.groups = []
         for cav in self.cavities:
             cav.close()
         self.cavities = []

@@ -8,18 +8,22 @@ from les_impulse3d_64_b200.ensemble import Ensemble
 pytestmark = pytest.mark.gpu
 
 
-def test_ensemble_matches_alone():
-    cases = workloads.ensemble_cases(count=6, seed=3, sizes=(12, 16, 24), re_range=(100.0, 2000.0))
-    for k, c in enumerate(cases):
-        c['precision'] = 'fp64' if k % 2 else 'mixed'
-    ens = Ensemble(cases)
+@pytest.mark.parametrize('batched', [True, False])
+def test_ensemble_matches_alone(batched):
+    """Batched (one graph per group of same-size cavities) or per-cavity stepping: bit-identical to each cavity
+    stepped alone."""
+    cases = workloads.ensemble_cases(count=9, seed=3, sizes=(12, 16, 24), re_range=(100.0, 2000.0))
+    for k, c in enumerate(cases):          # batches mixing uniform and stretched grids, in both forms
+        c['precision'] = 'mixed' if k < 5 else 'fp64'
+    ens = Ensemble(cases, batched=batched)
     try:
+        assert not batched or len(ens.batches) < len(cases)
         ens.advance(5, chunk=3)
         together = [ens.fields(i) for i in range(len(cases))]
     finally:
         ens.close()
-    for i in (0, 3, 5):
-        alone = Ensemble([cases[i]])
+    for i in (0, 3, 5, 8):
+        alone = Ensemble([cases[i]], batched=False)
         try:
             alone.advance(5, chunk=1)
             f = alone.fields(0)
