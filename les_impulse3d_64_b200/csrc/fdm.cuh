@@ -139,7 +139,7 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
     g.phi = phi;
     g.epilogue = epi;
     g.c = c;
-    const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch;
+    const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch * g_launch_batch;
     if (tiles64 >= 296) {
         dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
         if (!record_launch(kLkDgemm64, 0, grid, 0, g)) dgemm_mma_kernel<64, 64, 2, 2, 32><<<grid, 128, 0, st>>>(g);

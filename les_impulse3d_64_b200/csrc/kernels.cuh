@@ -37,6 +37,8 @@ struct LaunchRecord {
     std::vector<unsigned char> args;
 };
 inline thread_local std::vector<LaunchRecord>* g_launch_record = nullptr;
+// number of cavities the recorded launches will cover: tile choices that depend on the size of the grid use it
+inline thread_local int g_launch_batch = 1;
 template <class A> inline bool record_launch(int kind, int variant, dim3 grid, size_t smem, const A& a) {
     if (!g_launch_record) return false;
     const unsigned char* b = reinterpret_cast<const unsigned char*>(&a);

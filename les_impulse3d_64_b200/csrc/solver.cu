@@ -98,6 +98,8 @@ template <class T> class Solver : public SolverBase {
     // tile of the shared-memory sweep: 32 x TY x TZ cells (about 113 KB of shared memory in FP64, 85 KB in FP32)
     static constexpr int kTileTY = sizeof(T) == 8 ? 4 : 8;
     static constexpr int kTileTZ = 4;
+    static constexpr int kTileNT = sizeof(T) == 8 ? 256 : 512;     // threads: registers allow 512 in FP32
+    using TileG = TileGeom<kTileTY, kTileTZ, kTileNT>;
 
 public:
     explicit Solver(const CavityConfig& cfg) : c_(cfg) {
@@ -582,10 +584,10 @@ private:
         a.one_minus_r = (T)(1.0 - c_.reinit_r);
         a.nu = (T)c_.nu;
         if (tile_sweep_) {
-            using G = TileGeom<kTileTY, kTileTZ>;
+            using G = TileG;
             dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
             if (!record_launch(kLkSweep, 0, grid, G::template smem_bytes<T>(), a))
-                sweep_tile_kernel<T, kTileTY, kTileTZ><<<grid, kTileThreads, G::template smem_bytes<T>(), st>>>(a);
+                sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT><<<grid, kTileNT, G::template smem_bytes<T>(), st>>>(a);
         } else {
             dim3 grid(blocks_for(max_face_), 3);
             momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
@@ -720,9 +722,9 @@ private:
             // momentum sweep: the shared-memory tile kernel unless CAVITY_SWEEP=face
             const char* sw = std::getenv("CAVITY_SWEEP");
             tile_sweep_ = !(sw && std::string(sw) == "face");
-            using G = TileGeom<kTileTY, kTileTZ>;
+            using G = TileG;
             if (tile_sweep_)
-                check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ>,
+                check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::template smem_bytes<T>()));
             if (tc_fdm_) check(tc_transform_prepare());
         }
@@ -827,7 +829,7 @@ public:
 
 template <class T> class Batch : public BatchBase {
     using S_ = Solver<T>;
-    static constexpr int kTY = S_::kTileTY, kTZ = S_::kTileTZ;
+    static constexpr int kTY = S_::kTileTY, kTZ = S_::kTileTZ, kNT = S_::kTileNT;
 
 public:
     explicit Batch(const std::vector<S_*>& members) : m_(members) {
@@ -841,8 +843,8 @@ public:
         }
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
-        using G = TileGeom<kTY, kTZ>;
-        check(cudaFuncSetAttribute(sweep_tile_batched<T, kTY, kTZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        using G = TileGeom<kTY, kTZ, kNT>;
+        check(cudaFuncSetAttribute(sweep_tile_batched<T, kTY, kTZ, kNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)G::template smem_bytes<T>()));
         if (f.tc_fdm_) check(tc_transform_prepare_batched());
         for (int S = 0; S < 2; S++) build(S);
@@ -890,8 +892,14 @@ public:
 
 private:
     struct RecordGuard {
-        explicit RecordGuard(std::vector<LaunchRecord>* r) { g_launch_record = r; }
-        ~RecordGuard() { g_launch_record = nullptr; }
+        RecordGuard(std::vector<LaunchRecord>* r, int batch) {
+            g_launch_record = r;
+            g_launch_batch = batch;
+        }
+        ~RecordGuard() {
+            g_launch_record = nullptr;
+            g_launch_batch = 1;
+        }
     };
     // run `fn` on every member with a recorder installed, append the argument records of each recorded launch to
     // `host` (one contiguous array per launch) and, when `launch`, issue the batched launches on `st`
@@ -899,7 +907,7 @@ private:
         const size_t B = m_.size();
         std::vector<std::vector<LaunchRecord>> recs(B);
         for (size_t b = 0; b < B; b++) {
-            RecordGuard guard(&recs[b]);
+            RecordGuard guard(&recs[b], (int)B);
             fn(*m_[b]);
         }
         for (size_t b = 1; b < B; b++) {
@@ -924,7 +932,7 @@ private:
         const unsigned int per = r.grid.z;
         switch (r.kind) {
         case kLkStepBegin: step_begin_batched<<<dim3(1, 1, B), 32, 0, st>>>((const StepBeginArgs*)d); break;
-        case kLkSweep: sweep_tile_batched<T, kTY, kTZ><<<g, kTileThreads, r.smem, st>>>((const MomentumArgs<T>*)d, per); break;
+        case kLkSweep: sweep_tile_batched<T, kTY, kTZ, kNT><<<g, kNT, r.smem, st>>>((const MomentumArgs<T>*)d, per); break;
         case kLkStart: projection_start_batched<T><<<g, kThreads, 0, st>>>((const StartArgs<T>*)d); break;
         case kLkResidual: residual_batched<<<g, kThreads, 0, st>>>((const ResidualArgs*)d); break;
         case kLkFinish: finish_batched<T><<<g, kThreads, 0, st>>>((const FinishArgs<T>*)d); break;

@@ -19,11 +19,12 @@
 
 namespace cavity {
 
-constexpr int kTileThreads = 256;
-
-template <int TY, int TZ> struct TileGeom {
+// TY x TZ rows of 32 cells per CTA, NT threads (one warp per row at a time)
+template <int TY, int TZ, int NT> struct TileGeom {
     static constexpr int TX = 32;
-    static constexpr int ROWS_PER_THREAD = TY * TZ / 8;
+    static constexpr int THREADS = NT, WARPS = NT / 32;
+    static_assert(TY * TZ % WARPS == 0, "rows must divide among the warps");
+    static constexpr int ROWS_PER_THREAD = TY * TZ / WARPS;
     // velocity boxes: u on x-faces [x0-1, x0+TX+1] x cells [y0-3, y0+TY+2] x [z0-3, z0+TZ+2];
     // v on cells [x0-3, x0+TX+2] x y-faces [y0-1, y0+TY+1] x cells [z0-3, z0+TZ+2];
     // w on cells [x0-3, x0+TX+2] x [y0-3, y0+TY+2] x z-faces [z0-1, z0+TZ+1]
@@ -36,8 +37,8 @@ template <int TY, int TZ> struct TileGeom {
     static constexpr int NK = (TX + 1) * (TY + 1) * (TZ + 1);  // cells [x0-1, x0+TX) x [y0-1, y0+TY) x [z0-1, z0+TZ)
     // table slices: indices [lo-2, lo+T+2] of each axis
     static constexpr int SX = TX + 5, SY = TY + 5, SZ = TZ + 5;
-    static constexpr int NT = kNumTabs * (SX + SY + SZ);
-    static constexpr int ELEMS = NU + NV + NW + 3 * NM + NK + NT;
+    static constexpr int NTAB = kNumTabs * (SX + SY + SZ);
+    static constexpr int ELEMS = NU + NV + NW + 3 * NM + NK + NTAB;
     template <class T> static constexpr size_t smem_bytes() { return sizeof(T) * (size_t)ELEMS; }
 };
 
@@ -52,10 +53,10 @@ __device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* src) {
 
 // Stage a W x H x D box of a face array with extents (ex, ey, ez) and corner (xs, ys, zs), coordinates clamped
 // into the array.  Flattened over the CTA.  With `blend` the box receives r m + (1-r) u.
-template <class T, int W, int H, int D>
+template <class T, int W, int H, int D, int NT>
 __device__ __forceinline__ void stage_box(T* dst, const T* __restrict__ m, const T* __restrict__ u, bool blend, T r,
                                           T omr, int xs, int ys, int zs, int ex, int ey, int ez) {
-    for (int e = threadIdx.x; e < W * H * D; e += kTileThreads) {
+    for (int e = threadIdx.x; e < W * H * D; e += NT) {
         const int ix = e % W, rr = e / W, iy = rr % H, iz = rr / H;
         const long long gi = clampi(xs + ix, 0, ex - 1) +
                              (long long)ex * (clampi(ys + iy, 0, ey - 1) + (long long)ey * clampi(zs + iz, 0, ez - 1));
@@ -109,9 +110,9 @@ __device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* 
     return val;
 }
 
-template <class T, int TY, int TZ>
+template <class T, int TY, int TZ, int NT>
 __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
-    using G = TileGeom<TY, TZ>;
+    using G = TileGeom<TY, TZ, NT>;
     constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
     constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
     constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;      // plane strides of the velocity boxes
@@ -135,13 +136,13 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     const bool blend = a.stage == 0;
 
     // ---- stage
-    stage_box<T, UW, UH, G::UD>(SU, a.u[X], nullptr, false, T(0), T(0), x0 - 1, y0 - 3, z0 - 3, nx + 1, ny, nz);
-    stage_box<T, VW, VH, G::VD>(SV, a.u[Y], nullptr, false, T(0), T(0), x0 - 3, y0 - 1, z0 - 3, nx, ny + 1, nz);
-    stage_box<T, WW, WH, G::WD>(SW, a.u[Z], nullptr, false, T(0), T(0), x0 - 3, y0 - 3, z0 - 1, nx, ny, nz + 1);
-    stage_box<T, MW, MH, G::MD>(MX, a.m[X], a.u[X], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx + 1, ny, nz);
-    stage_box<T, MW, MH, G::MD>(MY, a.m[Y], a.u[Y], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny + 1, nz);
-    stage_box<T, MW, MH, G::MD>(MZ, a.m[Z], a.u[Z], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny, nz + 1);
-    for (int e = threadIdx.x; e < kNumTabs * (G::SX + G::SY + G::SZ); e += kTileThreads) {
+    stage_box<T, UW, UH, G::UD, NT>(SU, a.u[X], nullptr, false, T(0), T(0), x0 - 1, y0 - 3, z0 - 3, nx + 1, ny, nz);
+    stage_box<T, VW, VH, G::VD, NT>(SV, a.u[Y], nullptr, false, T(0), T(0), x0 - 3, y0 - 1, z0 - 3, nx, ny + 1, nz);
+    stage_box<T, WW, WH, G::WD, NT>(SW, a.u[Z], nullptr, false, T(0), T(0), x0 - 3, y0 - 3, z0 - 1, nx, ny, nz + 1);
+    stage_box<T, MW, MH, G::MD, NT>(MX, a.m[X], a.u[X], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx + 1, ny, nz);
+    stage_box<T, MW, MH, G::MD, NT>(MY, a.m[Y], a.u[Y], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny + 1, nz);
+    stage_box<T, MW, MH, G::MD, NT>(MZ, a.m[Z], a.u[Z], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny, nz + 1);
+    for (int e = threadIdx.x; e < kNumTabs * (G::SX + G::SY + G::SZ); e += NT) {
         int k, i, axis, len, lo;
         if (e < kNumTabs * G::SX) { axis = X; k = e / G::SX; i = e % G::SX; len = G::SX; lo = x0; }
         else if (e < kNumTabs * (G::SX + G::SY)) {
@@ -163,7 +164,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     const TabSlice<T, G::SZ> tZ{TZs, z0};
 
     // ---- K = u.m per cell (x0-1+ix, y0-1+iy, z0-1+iz)
-    for (int e = threadIdx.x; e < G::NK; e += kTileThreads) {
+    for (int e = threadIdx.x; e < G::NK; e += NT) {
         const int ix = e % (TX + 1), r = e / (TX + 1), iy = r % (TY + 1), iz = r / (TY + 1);
         const T* u0 = SU + ((iz + 2) * UH + iy + 2) * UW + ix;
         const T* v0 = SV + ((iz + 2) * VH + iy) * VW + 2 + ix;
@@ -186,7 +187,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
 
 #pragma unroll 1
     for (int k = 0; k < RPT; k++) {
-        const int row = warp + 8 * k, ry = row % TY, rz = row / TY;
+        const int row = warp + G::WARPS * k, ry = row % TY, rz = row / TY;
         const int x = x0 + lane, y = y0 + ry, z = z0 + rz;
         if (x >= nx || y >= ny || z >= nz) continue;
         const T* pu = SU + ((rz + 3) * UH + ry + 3) * UW + lane + 1;   // u at x-face x, cells (y, z)
@@ -342,18 +343,18 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     }
 }
 
-template <class T, int TY, int TZ>
-__global__ void __launch_bounds__(kTileThreads) sweep_tile_kernel(MomentumArgs<T> a) {
-    sweep_tile_body<T, TY, TZ>(a, real_blk());
+template <class T, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) sweep_tile_kernel(MomentumArgs<T> a) {
+    sweep_tile_body<T, TY, TZ, NT>(a, real_blk());
 }
 // a batch of cavities: grid z runs over cavities x `per` z-tiles
-template <class T, int TY, int TZ>
-__global__ void __launch_bounds__(kTileThreads) sweep_tile_batched(const MomentumArgs<T>* args, unsigned int per) {
+template <class T, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) sweep_tile_batched(const MomentumArgs<T>* args, unsigned int per) {
     __shared__ MomentumArgs<T> a;
     int cav;
     const Blk k = batch_blk(per, cav);
     load_args(a, args + cav);
-    sweep_tile_body<T, TY, TZ>(a, k);
+    sweep_tile_body<T, TY, TZ, NT>(a, k);
 }
 
 }  // namespace cavity

@@ -507,7 +507,7 @@ template <int BN> inline void launch_tc_bn(cudaStream_t st, const TcTransformArg
 // variant code of a recorded launch: tile width, field-is-A, fp64 field
 inline int tc_variant(int bn, const TcTransformArgs& g) { return bn | (g.field_is_a ? 1 << 8 : 0) | (g.field64 ? 1 << 9 : 0); }
 inline void launch_tc_transform(cudaStream_t st, const TcTransformArgs& g, int batch, int sms) {
-    const int bn = tc_pick_bn(g.M, g.N, batch, sms);
+    const int bn = tc_pick_bn(g.M, g.N, batch * g_launch_batch, sms);
     const dim3 grid((g.N + bn - 1) / bn, (g.M + kTcRows - 1) / kTcRows, batch);
     if (record_launch(kLkTc, tc_variant(bn, g), grid, (size_t)(bn == 128 ? TcSmem<128>::kBytes : bn == 64 ? TcSmem<64>::kBytes
                                                                                                        : TcSmem<32>::kBytes), g))
