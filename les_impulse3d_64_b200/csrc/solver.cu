@@ -413,6 +413,16 @@ private:
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         sms_ = sms;
         cell_blocks_ = (unsigned int)std::min<long long>(blocks_for(n_cell_), 4LL * sms);
+        // the grid-stride cell kernels: as many CTAs as fit on the device at once (latency-bound loads want every
+        // resident warp), and never more than one cell per thread
+        auto resident = [&](const void* fn) {
+            int per_sm = 4;
+            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
+            return (unsigned int)std::min<long long>(blocks_for(n_cell_), (long long)std::max(per_sm, 1) * sms);
+        };
+        start_blocks_ = resident((const void*)projection_start_kernel<T>);
+        residual_blocks_ = resident((const void*)residual_kernel);
+        finish_blocks_ = resident((const void*)finish_kernel<T>);
         if (tc_fdm_) {
             inv_lambda_f_ = arena_.alloc<float>(n_cell_);
             const int n[3] = {nx_, ny_, nz_};
@@ -561,6 +571,9 @@ private:
     }
 
     // ------------------------------------------------------------------------------ kernel launches
+    // grid of a recorded cell kernel: in a batch the launch already spans many cavities, so each cavity keeps
+    // the smaller grid (fewer partials per reduction)
+    unsigned int cell_grid(unsigned int alone) const { return g_launch_batch > 1 ? cell_blocks_ : alone; }
     void launch_step_begin(cudaStream_t st) {
         StepBeginArgs a;
         a.p = p_;
@@ -614,7 +627,7 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        if (!record_launch(kLkStart, 0, dim3(cell_blocks_), 0, a)) projection_start_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkStart, 0, dim3(cell_grid(start_blocks_)), 0, a)) projection_start_kernel<T><<<start_blocks_, kThreads, 0, st>>>(a);
     }
     void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, int use_h) {
         ResidualArgs a;
@@ -627,7 +640,7 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        if (!record_launch(kLkResidual, 0, dim3(cell_blocks_), 0, a)) residual_kernel<<<cell_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkResidual, 0, dim3(cell_grid(residual_blocks_)), 0, a)) residual_kernel<<<residual_blocks_, kThreads, 0, st>>>(a);
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
@@ -654,7 +667,7 @@ private:
         a.stage = stage;
         a.c = ctrl_;
         a.partial = partial_;
-        if (!record_launch(kLkFinish, 0, dim3(cell_blocks_), 0, a)) finish_kernel<T><<<cell_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkFinish, 0, dim3(cell_grid(finish_blocks_)), 0, a)) finish_kernel<T><<<finish_blocks_, kThreads, 0, st>>>(a);
     }
 
     // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
@@ -797,7 +810,8 @@ private:
     TcFdmOperands tcop_ = {};
     double* partial_;
     long long partial_blocks_;
-    unsigned int cell_blocks_ = 1;     // grid of the grid-stride cell kernels: at most 4 CTAs per SM
+    unsigned int cell_blocks_ = 1;     // grid of other grid-stride cell kernels: at most 4 CTAs per SM
+    unsigned int start_blocks_ = 1, residual_blocks_ = 1, finish_blocks_ = 1;
     Control* ctrl_;
     double *slots_, *stats_, *line_, *dstage_[2];
     unsigned int* out_counters_;
