@@ -42,6 +42,9 @@ def parse_args():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--count', type=int, default=256, help='cavities of the c4_ensemble workload')
     ap.add_argument('--chunk', type=int, default=8, help='steps queued per cavity between waits (ensemble)')
+    ap.add_argument('--requests', type=int, default=64, help='requests of the c5_serving stream')
+    ap.add_argument('--rate', type=float, default=50.0, help='Poisson arrival rate (1/s) of c5_serving')
+    ap.add_argument('--t-end', type=float, default=0.1, help='simulated end time of each c5_serving request')
     return ap.parse_args()
 
 
@@ -331,6 +334,30 @@ def run_ensemble(args, ranks):
     }
 
 
+def run_serving(args, ranks):
+    """C5: a seeded Poisson stream of cavity requests served in real time by the batched mixed-form server,
+    then by the plain FP64 form one request at a time; p50 / p99 time to solution of each."""
+    from les_impulse3d_64_b200.serve import Server, serving_requests, summary
+    reqs = serving_requests(args.requests, args.rate, seed=0, t_end=args.t_end, with_fields=True)
+    ranks.barrier()
+    with ClockSampler(ranks.local) as clocks:
+        ours = summary(Server(budget_bytes=120e9, precision=args.precision or 'mixed', chunk=args.chunk).run(reqs))
+    plain = summary(Server(budget_bytes=120e9, precision='fp64', chunk=args.chunk, batched=False,
+                           max_running=1).run(reqs))
+    p99 = ranks.max(ours['p99_s'])
+    return {
+        'metric': 'p99 time-to-solution', 'value': p99, 'unit': 's', 'n_gpus': ranks.world, 'steps': None,
+        'warmup': 0, 'ms_per_step': None, 'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if (args.precision or 'mixed') == 'mixed' else 'f64',
+        'data': 'synthetic (seeded Poisson request stream, numpy default_rng)',
+        'config': {'workload': 'c5_serving', 'requests': args.requests, 'rate_per_s': args.rate,
+                   't_end': args.t_end, 'sizes': '32^3, 64^3, 64x64x128, 96^3, 128^3', 'budget_bytes': 120e9,
+                   'chunk': args.chunk, 'parallelism': f'replicas x{ranks.world}'},
+        'serving': ours, 'plain_fp64_one_at_a_time': plain,
+        'clocks': clocks.summary(),
+    }
+
+
 def run_reference(args, ranks):
     if ranks.rank != 0:
         return None
@@ -362,6 +389,8 @@ def main():
             line = run_reference(args, ranks)
         elif args.workload == 'c4_ensemble':
             line = run_ensemble(args, ranks)
+        elif args.workload == 'c5_serving':
+            line = run_serving(args, ranks)
         else:
             line = run_ours(args, ranks)
         if line is not None and ranks.rank == 0:

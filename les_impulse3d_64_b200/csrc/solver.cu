@@ -37,28 +37,51 @@ static void check(cudaError_t e) {
 static unsigned int blocks_for(long long n) { return (unsigned int)((n + kThreads - 1) / kThreads); }
 
 // ------------------------------------------------------------------------------------------ device memory
+// Device memory of one solver: a block reserved up front (one cudaMalloc, zero-filled once) from which the
+// arrays are carved at 256-byte alignment, and separate zero-filled allocations for anything beyond it.  One
+// allocation instead of dozens keeps creating and destroying a solver cheap when many come and go (serving).
 class DeviceArena {
 public:
     ~DeviceArena() { release(); }
+    void reserve(size_t bytes) {
+        bytes = (bytes + 255) / 256 * 256;
+        check(cudaMalloc(&block_, bytes));
+        check(cudaMemset(block_, 0, bytes));
+        ptrs_.push_back(block_);
+        cap_ = bytes;
+        used_ = 0;
+    }
     template <class T> T* alloc(long long n) {
-        void* p = nullptr;
         const size_t bytes = sizeof(T) * (size_t)std::max(n, 1LL);
+        bytes_ += bytes;
+        const size_t need = (bytes + 255) / 256 * 256;
+        if (block_ && used_ + need <= cap_) {
+            void* p = static_cast<char*>(block_) + used_;
+            used_ += need;
+            return (T*)p;
+        }
+        void* p = nullptr;
         check(cudaMalloc(&p, bytes));
         check(cudaMemset(p, 0, bytes));
         ptrs_.push_back(p);
-        bytes_ += bytes;
         return (T*)p;
     }
     void release() {
         for (void* p : ptrs_) cudaFree(p);
         ptrs_.clear();
+        block_ = nullptr;
+        cap_ = used_ = 0;
         bytes_ = 0;
     }
     long long bytes() const { return bytes_; }
 private:
     std::vector<void*> ptrs_;
+    void* block_ = nullptr;
+    size_t cap_ = 0, used_ = 0;
     long long bytes_ = 0;
 };
+
+static long long estimate_bytes(const CavityConfig& c, int precision);
 
 class SolverBase {
 public:
@@ -116,6 +139,7 @@ public:
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
         setup_params();
+        arena_.reserve((size_t)estimate_bytes(c_, sizeof(T) == 8 ? 0 : 1));
         {
             // Mixed form: FDM transforms on the tcgen05 tensor cores (3xTF32) from 128^3 cells up, FP64 DMMA
             // transforms below.  FP32 transforms need two refinement passes where FP64 ones need one, which
@@ -162,6 +186,7 @@ public:
     }
 
     void step_async(int count) override {
+        ensure_graphs(false);
         if (pending_.empty()) steps_before_ = hc_.steps;
         for (int i = 0; i < count; i++) {
             if (eager_) enqueue_step(par_, false, true);
@@ -345,6 +370,7 @@ public:
 
     void time_steps(int warmup, int steps, int flush, float* ms, float* kms) override {
         if (flush && !flush_) check(cudaMalloc(&flush_, kFlushBytes));
+        ensure_graphs(true);
         for (int i = 0; i < warmup; i++) step(nullptr);
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0));
@@ -492,9 +518,9 @@ private:
                 }
         check(cudaMemcpy(inv_lambda_, inv.data(), sizeof(double) * n_cell_, cudaMemcpyHostToDevice));
         // The arena's zero-fills and these uploads run on the legacy default stream, and a copy from pageable
-        // memory may return before its DMA has landed; stream_ is non-blocking, so wait for all of it before
-        // kernels on stream_ read the uploaded operators.
-        check(cudaDeviceSynchronize());
+        // memory may return before its DMA has landed; stream_ is non-blocking, so wait for that stream before
+        // kernels on stream_ read the uploaded operators (only for it: other solvers' streams keep running).
+        check(cudaStreamSynchronize(cudaStreamLegacy));
         if (tc_fdm_) {
             // float S and 1/lambda as the reference keeps them (backend.cu:766-786), S split into hi/lo TF32
             // images of its rows (img 0, 1) and of its columns = rows of S^T (img 2, 3)
@@ -514,7 +540,7 @@ private:
         fdm_.inv_lambda = inv_lambda_;
         const std::vector<int> cells = probe_cells(c_, ax_);
         if (!cells.empty()) check(cudaMemcpy(probe_cells_, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
-        check(cudaDeviceSynchronize());
+        check(cudaStreamSynchronize(cudaStreamLegacy));
         push_control();
     }
 
@@ -744,16 +770,20 @@ private:
         for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
         const char* env = std::getenv("CAVITY_GRAPHS");
         eager_ = env && env[0] == '0';
+    }
+    // the step graphs of both state parities (timing: with events around the sweeps), captured on first use, so
+    // a solver that only takes part in batches or is only initialised never builds them
+    void ensure_graphs(bool timing) {
         if (eager_) return;
-        for (int S = 0; S < 2; S++)
-            for (int timing = 0; timing < 2; timing++) {
-                cudaGraph_t& g = timing ? tgraph_[S] : graph_[S];
-                cudaGraphExec_t& ex = timing ? texec_[S] : exec_[S];
-                check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-                enqueue_step(S, timing, false);
-                check(cudaStreamEndCapture(stream_, &g));
-                check(cudaGraphInstantiate(&ex, g, 0));
-            }
+        for (int S = 0; S < 2; S++) {
+            cudaGraph_t& g = timing ? tgraph_[S] : graph_[S];
+            cudaGraphExec_t& ex = timing ? texec_[S] : exec_[S];
+            if (ex) continue;
+            check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(S, timing, false);
+            check(cudaStreamEndCapture(stream_, &g));
+            check(cudaGraphInstantiate(&ex, g, 0));
+        }
     }
 
     // A projection outside a step (initialize, kick): m -> u, phi from no guess (backend.cu:849-854), with
