@@ -39,6 +39,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // flight at once (cp.async, zero-filled outside the matrices).
 template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
 __device__ void dgemm_mma_body(const GemmArgs<double>& g, const Blk& blk, bool first) {
+    pdl_launch_dependents();
+    pdl_wait();
     constexpr int NT = WARPS_M * WARPS_N * 32;
     constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;     // warp tile
     constexpr int FM = WTM / 8, FN = WTN / 8;                   // fragments per warp tile
@@ -142,10 +144,10 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
     const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch * g_launch_batch;
     if (tiles64 >= 296) {
         dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
-        if (!record_launch(kLkDgemm64, 0, grid, 0, g)) dgemm_mma_kernel<64, 64, 2, 2, 32><<<grid, 128, 0, st>>>(g);
+        if (!record_launch(kLkDgemm64, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<64, 64, 2, 2, 32>, grid, dim3(128), 0, st, g);
     } else {
         dim3 grid((N + 31) / 32, (M + 31) / 32, batch);
-        if (!record_launch(kLkDgemm32, 0, grid, 0, g)) dgemm_mma_kernel<32, 32, 2, 2, 64><<<grid, 128, 0, st>>>(g);
+        if (!record_launch(kLkDgemm32, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<32, 32, 2, 2, 64>, grid, dim3(128), 0, st, g);
     }
 }
 

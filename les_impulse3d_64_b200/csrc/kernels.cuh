@@ -39,6 +39,23 @@ struct LaunchRecord {
 inline thread_local std::vector<LaunchRecord>* g_launch_record = nullptr;
 // number of cavities the recorded launches will cover: tile choices that depend on the size of the grid use it
 inline thread_local int g_launch_batch = 1;
+// launch a step kernel with programmatic stream serialization (see pdl_wait); inside a stream capture this makes
+// the graph edge to the previous kernel a programmatic one
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 template <class A> inline bool record_launch(int kind, int variant, dim3 grid, size_t smem, const A& a) {
     if (!g_launch_record) return false;
     const unsigned char* b = reinterpret_cast<const unsigned char*>(&a);
@@ -175,6 +192,12 @@ __device__ __forceinline__ Blk batch_blk(unsigned int per, int& cavity) {
     return {blockIdx.x, blockIdx.y, blockIdx.z % per, gridDim.x, gridDim.y, per};
 }
 __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0; }
+// Programmatic dependent launch: the step kernels are launched so that the next kernel may start while this one
+// finishes.  Every step kernel lets its dependents launch at entry and waits for its predecessor to complete
+// (with all its memory visible) before it reads anything a predecessor wrote.  Both are no-ops for a kernel
+// launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 // copy a cavity's kernel arguments into shared memory (the whole block, then a barrier)
 template <class A> __device__ __forceinline__ void load_args(A& dst, const A* src) {
     static_assert(sizeof(A) % 4 == 0, "argument records are copied in words");
@@ -234,6 +257,8 @@ struct StepBeginArgs {
     Control* c;
 };
 __device__ void step_begin_body(const Params& p, Control* c) {
+    pdl_launch_dependents();
+    pdl_wait();
     if (threadIdx.x != 0) return;
     if (c->error) return;          // an earlier queued step failed: leave everything as it is
     const double rates[2] = {(double)(float)c->cfl_rate, p.viscous_rate};
@@ -378,6 +403,8 @@ __device__ __forceinline__ void decide_loop(const Params& p, Control* c, cudaGra
 
 template <class T>
 __device__ void projection_start_body(const StartArgs<T>& a, const Blk& k) {
+    pdl_launch_dependents();
+    pdl_wait();
     Control* c = a.c;
     const Params& p = a.p;
     const int err = c->error;
@@ -498,6 +525,8 @@ struct ResidualArgs {
 
 // A cavity whose refinement loop has ended (a batch runs passes while any cavity needs one) skips the pass.
 __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
+    pdl_launch_dependents();
+    pdl_wait();
     Control* c = a.c;
     if (!c->cond) return;
     const Params& p = a.p;
@@ -601,6 +630,8 @@ template <class T> struct FinishArgs {
 
 template <class T>
 __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
+    pdl_launch_dependents();
+    pdl_wait();
     Control* c = a.c;
     const Params& p = a.p;
     const int err = c->error;

@@ -604,7 +604,7 @@ private:
         StepBeginArgs a;
         a.p = p_;
         a.c = ctrl_;
-        if (!record_launch(kLkStepBegin, 0, dim3(1), 0, a)) step_begin_kernel<<<1, 32, 0, st>>>(p_, ctrl_);
+        if (!record_launch(kLkStepBegin, 0, dim3(1), 0, a)) check(launch_pdl(step_begin_kernel, dim3(1), dim3(32), 0, st, p_, ctrl_));
     }
     void launch_momentum(cudaStream_t st, int stage, int S, int in, int out) {
         MomentumArgs<T> a;
@@ -626,7 +626,8 @@ private:
             using G = TileG;
             dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
             if (!record_launch(kLkSweep, 0, grid, G::template smem_bytes<T>(), a))
-                sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT><<<grid, kTileNT, G::template smem_bytes<T>(), st>>>(a);
+                check(launch_pdl(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>, grid, dim3(kTileNT),
+                                 G::template smem_bytes<T>(), st, a));
         } else {
             dim3 grid(blocks_for(max_face_), 3);
             momentum_kernel<T><<<grid, kThreads, 0, st>>>(a);
@@ -653,7 +654,8 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        if (!record_launch(kLkStart, 0, dim3(cell_grid(start_blocks_)), 0, a)) projection_start_kernel<T><<<start_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkStart, 0, dim3(cell_grid(start_blocks_)), 0, a))
+            check(launch_pdl(projection_start_kernel<T>, dim3(start_blocks_), dim3(kThreads), 0, st, a));
     }
     void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, int use_h) {
         ResidualArgs a;
@@ -666,7 +668,8 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        if (!record_launch(kLkResidual, 0, dim3(cell_grid(residual_blocks_)), 0, a)) residual_kernel<<<residual_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkResidual, 0, dim3(cell_grid(residual_blocks_)), 0, a))
+            check(launch_pdl(residual_kernel, dim3(residual_blocks_), dim3(kThreads), 0, st, a));
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
@@ -693,7 +696,8 @@ private:
         a.stage = stage;
         a.c = ctrl_;
         a.partial = partial_;
-        if (!record_launch(kLkFinish, 0, dim3(cell_grid(finish_blocks_)), 0, a)) finish_kernel<T><<<finish_blocks_, kThreads, 0, st>>>(a);
+        if (!record_launch(kLkFinish, 0, dim3(cell_grid(finish_blocks_)), 0, a))
+            check(launch_pdl(finish_kernel<T>, dim3(finish_blocks_), dim3(kThreads), 0, st, a));
     }
 
     // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
@@ -975,13 +979,19 @@ private:
         const dim3 g(r.grid.x, r.grid.y, r.grid.z * B);
         const unsigned int per = r.grid.z;
         switch (r.kind) {
-        case kLkStepBegin: step_begin_batched<<<dim3(1, 1, B), 32, 0, st>>>((const StepBeginArgs*)d); break;
-        case kLkSweep: sweep_tile_batched<T, kTY, kTZ, kNT><<<g, kNT, r.smem, st>>>((const MomentumArgs<T>*)d, per); break;
-        case kLkStart: projection_start_batched<T><<<g, kThreads, 0, st>>>((const StartArgs<T>*)d); break;
-        case kLkResidual: residual_batched<<<g, kThreads, 0, st>>>((const ResidualArgs*)d); break;
-        case kLkFinish: finish_batched<T><<<g, kThreads, 0, st>>>((const FinishArgs<T>*)d); break;
-        case kLkDgemm64: dgemm_mma_batched<64, 64, 2, 2, 32><<<g, 128, 0, st>>>((const GemmArgs<double>*)d, per); break;
-        case kLkDgemm32: dgemm_mma_batched<32, 32, 2, 2, 64><<<g, 128, 0, st>>>((const GemmArgs<double>*)d, per); break;
+        case kLkStepBegin: check(launch_pdl(step_begin_batched, dim3(1, 1, B), dim3(32), 0, st, (const StepBeginArgs*)d)); break;
+        case kLkSweep:
+            check(launch_pdl(sweep_tile_batched<T, kTY, kTZ, kNT>, g, dim3(kNT), r.smem, st, (const MomentumArgs<T>*)d, per));
+            break;
+        case kLkStart: check(launch_pdl(projection_start_batched<T>, g, dim3(kThreads), 0, st, (const StartArgs<T>*)d)); break;
+        case kLkResidual: check(launch_pdl(residual_batched, g, dim3(kThreads), 0, st, (const ResidualArgs*)d)); break;
+        case kLkFinish: check(launch_pdl(finish_batched<T>, g, dim3(kThreads), 0, st, (const FinishArgs<T>*)d)); break;
+        case kLkDgemm64:
+            check(launch_pdl(dgemm_mma_batched<64, 64, 2, 2, 32>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, per));
+            break;
+        case kLkDgemm32:
+            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 2, 64>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, per));
+            break;
         case kLkTc: launch_tc_batched(r.variant, g, per, (const TcTransformArgs*)d, st); break;
         default: fail("batch: unknown launch");
         }

@@ -113,6 +113,8 @@ __device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* 
 template <class T, int TY, int TZ, int NT>
 __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     using G = TileGeom<TY, TZ, NT>;
+    pdl_launch_dependents();
+    pdl_wait();
     constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
     constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
     constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;      // plane strides of the velocity boxes

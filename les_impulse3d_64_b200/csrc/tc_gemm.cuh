@@ -214,17 +214,15 @@ __device__ void tc_transform_body(const TcTransformArgs& g, const Blk& blk, bool
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base;
     __shared__ int failed;
-    if (g.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(g.handle, 0u);
-    // the control block is read while TMEM and the barriers are set up
-    const Control* c = g.c;
-    const int err = c->error, use_rhs = c->use_rhs, reset = c->reset_phi, cond = c->cond;
-    const double rhs2 = c->rhs_norm2, res2 = c->res_norm2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
     const int b = blk.z;
     const int m0 = blk.y * kTcRows, n0 = blk.x * BN;
     const int row = m0 + warp * 32 + lane;
     const uint32_t sbase = smem_addr(smem);
     constexpr uint32_t kCols = BN < 32 ? 32 : BN;
+    // TMEM and the barriers are set up while the previous kernel finishes (programmatic dependent launch); at
+    // most two CTAs of this kernel and two of a preceding one share an SM, within its 512 TMEM columns
+    pdl_launch_dependents();
     if (warp == 0) tmem_alloc(&tmem_base, kCols);
     if (tid == 0) {
         mbar_init(&mbar[0], 1);
@@ -236,6 +234,11 @@ __device__ void tc_transform_body(const TcTransformArgs& g, const Blk& blk, bool
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base;
+    pdl_wait();
+    if (g.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(g.handle, 0u);
+    const Control* c = g.c;
+    const int err = c->error, use_rhs = c->use_rhs, reset = c->reset_phi, cond = c->cond;
+    const double rhs2 = c->rhs_norm2, res2 = c->res_norm2;
     const double r2 = use_rhs ? rhs2 : res2;
     // failed, this cavity's refinement has ended, or a zero residual: no pass (backend.cu:803-804)
     if (err || !cond || !(r2 > 0)) {
@@ -482,9 +485,10 @@ inline cudaError_t tc_transform_prepare_batched() {
 }
 template <int BN>
 inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
-    if (fa && f64) tc_transform_batched<BN, 1, 1><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(d, per);
-    else if (fa) tc_transform_batched<BN, 1, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(d, per);
-    else tc_transform_batched<BN, 0, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(d, per);
+    const dim3 block(kTcThreads);
+    if (fa && f64) launch_pdl(tc_transform_batched<BN, 1, 1>, grid, block, TcSmem<BN>::kBytes, st, d, per);
+    else if (fa) launch_pdl(tc_transform_batched<BN, 1, 0>, grid, block, TcSmem<BN>::kBytes, st, d, per);
+    else launch_pdl(tc_transform_batched<BN, 0, 0>, grid, block, TcSmem<BN>::kBytes, st, d, per);
 }
 // a recorded launch (variant: see tc_variant) over a batch of cavities
 inline void launch_tc_batched(int variant, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
@@ -500,9 +504,10 @@ inline cudaError_t tc_transform_prepare() {
     return e;
 }
 template <int BN> inline void launch_tc_bn(cudaStream_t st, const TcTransformArgs& g, dim3 grid) {
-    if (g.field_is_a && g.field64) tc_transform_kernel<BN, 1, 1><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
-    else if (g.field_is_a) tc_transform_kernel<BN, 1, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
-    else tc_transform_kernel<BN, 0, 0><<<grid, kTcThreads, TcSmem<BN>::kBytes, st>>>(g);
+    const dim3 block(kTcThreads);
+    if (g.field_is_a && g.field64) launch_pdl(tc_transform_kernel<BN, 1, 1>, grid, block, TcSmem<BN>::kBytes, st, g);
+    else if (g.field_is_a) launch_pdl(tc_transform_kernel<BN, 1, 0>, grid, block, TcSmem<BN>::kBytes, st, g);
+    else launch_pdl(tc_transform_kernel<BN, 0, 0>, grid, block, TcSmem<BN>::kBytes, st, g);
 }
 // variant code of a recorded launch: tile width, field-is-A, fp64 field
 inline int tc_variant(int bn, const TcTransformArgs& g) { return bn | (g.field_is_a ? 1 << 8 : 0) | (g.field64 ? 1 << 9 : 0); }
