@@ -51,17 +51,30 @@ __device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* src) {
     else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
 }
 
-// Stage a W x H x D box of a face array with extents (ex, ey, ez) and corner (xs, ys, zs), coordinates clamped
-// into the array.  Flattened over the CTA.  With `blend` the box receives r m + (1-r) u.
+// Global offsets of the rows (y, z) of a W x H x D box of a face array with extents (ex, ey, ez) whose corner is
+// (., ys, zs), clamped into the array; rows are numbered iy + H * iz.
+template <int H, int D>
+__device__ __forceinline__ int box_row_base(int row, int ys, int zs, int ex, int ey, int ez) {
+    const int iy = row % H, iz = row / H;
+    return ex * (clampi(ys + iy, 0, ey - 1) + ey * clampi(zs + iz, 0, ez - 1));
+}
+
+// Stage a W x H x D box of a face array whose x-extent is ex and corner x is xs, coordinates clamped into the
+// array, from the row offsets `rowbase` (box_row_base).  Each thread keeps one column (its x offset and clamp)
+// and steps through the rows NT / W at a time.  With `blend` the box receives r m + (1-r) u.
 template <class T, int W, int H, int D, int NT>
-__device__ __forceinline__ void stage_box(T* dst, const T* __restrict__ m, const T* __restrict__ u, bool blend, T r,
-                                          T omr, int xs, int ys, int zs, int ex, int ey, int ez) {
-    for (int e = threadIdx.x; e < W * H * D; e += NT) {
-        const int ix = e % W, rr = e / W, iy = rr % H, iz = rr / H;
-        const long long gi = clampi(xs + ix, 0, ex - 1) +
-                             (long long)ex * (clampi(ys + iy, 0, ey - 1) + (long long)ey * clampi(zs + iz, 0, ez - 1));
-        if (blend) dst[e] = r * m[gi] + omr * u[gi];
-        else cp_async_elem<sizeof(T)>(dst + e, m + gi);
+__device__ __forceinline__ void stage_box(T* dst, const int* rowbase, const T* __restrict__ m, const T* __restrict__ u,
+                                          bool blend, T r, T omr, int xs, int ex) {
+    constexpr int RPS = NT / W, ROWS = H * D;
+    const int t = threadIdx.x;
+    if (t >= RPS * W) return;
+    const int ix = t % W;
+    const int gx = clampi(xs + ix, 0, ex - 1);
+    for (int row = t / W; row < ROWS; row += RPS) {
+        const int gi = rowbase[row] + gx;
+        T* d = dst + row * W + ix;
+        if (blend) *d = r * m[gi] + omr * u[gi];
+        else cp_async_elem<sizeof(T)>(d, m + gi);
     }
 }
 
@@ -137,13 +150,28 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     const int o4 = p.o4;
     const bool blend = a.stage == 0;
 
-    // ---- stage
-    stage_box<T, UW, UH, G::UD, NT>(SU, a.u[X], nullptr, false, T(0), T(0), x0 - 1, y0 - 3, z0 - 3, nx + 1, ny, nz);
-    stage_box<T, VW, VH, G::VD, NT>(SV, a.u[Y], nullptr, false, T(0), T(0), x0 - 3, y0 - 1, z0 - 3, nx, ny + 1, nz);
-    stage_box<T, WW, WH, G::WD, NT>(SW, a.u[Z], nullptr, false, T(0), T(0), x0 - 3, y0 - 3, z0 - 1, nx, ny, nz + 1);
-    stage_box<T, MW, MH, G::MD, NT>(MX, a.m[X], a.u[X], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx + 1, ny, nz);
-    stage_box<T, MW, MH, G::MD, NT>(MY, a.m[Y], a.u[Y], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny + 1, nz);
-    stage_box<T, MW, MH, G::MD, NT>(MZ, a.m[Z], a.u[Z], blend, a.r, a.one_minus_r, x0 - 1, y0 - 1, z0 - 1, nx, ny, nz + 1);
+    // ---- stage: row offsets of the six boxes first (one pass), then every box
+    constexpr int RU = G::UH * G::UD, RV = G::VH * G::VD, RW = G::WH * G::WD, RM = G::MH * G::MD;
+    __shared__ int rowbase[RU + RV + RW + 3 * RM];
+    for (int e = threadIdx.x; e < RU + RV + RW + 3 * RM; e += NT) {
+        int v;
+        if (e < RU) v = box_row_base<G::UH, G::UD>(e, y0 - 3, z0 - 3, nx + 1, ny, nz);
+        else if (e < RU + RV) v = box_row_base<G::VH, G::VD>(e - RU, y0 - 1, z0 - 3, nx, ny + 1, nz);
+        else if (e < RU + RV + RW) v = box_row_base<G::WH, G::WD>(e - RU - RV, y0 - 3, z0 - 1, nx, ny, nz + 1);
+        else {
+            const int f = e - RU - RV - RW, comp = f / RM;
+            v = box_row_base<G::MH, G::MD>(f % RM, y0 - 1, z0 - 1, nx + (comp == X), ny + (comp == Y), nz + (comp == Z));
+        }
+        rowbase[e] = v;
+    }
+    __syncthreads();
+    const int* rbm = rowbase + RU + RV + RW;
+    stage_box<T, UW, UH, G::UD, NT>(SU, rowbase, a.u[X], nullptr, false, T(0), T(0), x0 - 1, nx + 1);
+    stage_box<T, VW, VH, G::VD, NT>(SV, rowbase + RU, a.u[Y], nullptr, false, T(0), T(0), x0 - 3, nx);
+    stage_box<T, WW, WH, G::WD, NT>(SW, rowbase + RU + RV, a.u[Z], nullptr, false, T(0), T(0), x0 - 3, nx);
+    stage_box<T, MW, MH, G::MD, NT>(MX, rbm, a.m[X], a.u[X], blend, a.r, a.one_minus_r, x0 - 1, nx + 1);
+    stage_box<T, MW, MH, G::MD, NT>(MY, rbm + RM, a.m[Y], a.u[Y], blend, a.r, a.one_minus_r, x0 - 1, nx);
+    stage_box<T, MW, MH, G::MD, NT>(MZ, rbm + 2 * RM, a.m[Z], a.u[Z], blend, a.r, a.one_minus_r, x0 - 1, nx);
     for (int e = threadIdx.x; e < kNumTabs * (G::SX + G::SY + G::SZ); e += NT) {
         int k, i, axis, len, lo;
         if (e < kNumTabs * G::SX) { axis = X; k = e / G::SX; i = e % G::SX; len = G::SX; lo = x0; }
@@ -166,8 +194,9 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     const TabSlice<T, G::SZ> tZ{TZs, z0};
 
     // ---- K = u.m per cell (x0-1+ix, y0-1+iy, z0-1+iz)
-    for (int e = threadIdx.x; e < G::NK; e += NT) {
-        const int ix = e % (TX + 1), r = e / (TX + 1), iy = r % (TY + 1), iz = r / (TY + 1);
+    constexpr int KW = TX + 1, KRPS = NT / KW;
+    for (int e = threadIdx.x % KW + KW * (threadIdx.x / KW); threadIdx.x < KRPS * KW && e < G::NK; e += KRPS * KW) {
+        const int ix = threadIdx.x % KW, r = e / KW, iy = r % (TY + 1), iz = r / (TY + 1);
         const T* u0 = SU + ((iz + 2) * UH + iy + 2) * UW + ix;
         const T* v0 = SV + ((iz + 2) * VH + iy) * VW + 2 + ix;
         const T* w0 = SW + (iz * WH + iy + 2) * WW + 2 + ix;
