@@ -57,7 +57,7 @@ C2 = dict(name='c2_64cube_re1000', settings=settings(64, 1000.0, beta=1.5, cfl=0
 C3 = dict(name='c3_128cube_re3200', settings=settings(128, 3200.0, beta=2.0, cfl=0.5), steps=1000, noise=1e-3,
           seed=0, kicks=(), stats_from=None, precision='mixed', beta=2.0)
 
-# 256^3 stretched (beta 2.0), Re 3200, mixed: the size at which the stencil kernels' HBM roofline is judged
+# 256^3 stretched (beta 2.0), Re 3200, mixed: the size at which the stencil kernels' HBM roofline is measured
 C6 = dict(name='c6_256cube_re3200', settings=settings(256, 3200.0, beta=2.0, cfl=0.5), steps=100, noise=1e-3,
           seed=0, kicks=(), stats_from=None, precision='mixed', beta=2.0)
 
