@@ -81,6 +81,9 @@ int cavity_step_async(CavitySolver* s, int count);
 int cavity_sync(CavitySolver* s, CavityReport* report);
 int cavity_get_field(CavitySolver* s, int field, void* out);
 int cavity_set_field(CavitySolver* s, int field, const void* in);
+/* Handle forms of solver_report and solver_set_clock (backend.cu:1092-1094, 1156-1158). */
+int cavity_report(CavitySolver* s, CavityReport* r);
+int cavity_set_clock(CavitySolver* s, double t, long long steps, double last_dt);
 int cavity_probes(CavitySolver* s, float* out);
 int cavity_diagnostics(CavitySolver* s, CavityDiagnostics* d);
 /* Device bytes this cavity holds (state, work arrays, pressure tables), for admission control. */
@@ -97,6 +100,16 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 CavitySolver* cavity_default(void);
 /* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */
 int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
+/* Checkpoints (no counterpart in the reference, whose restart through solver_set_field drops the potential
+ * history and the dt lag, backend.cu:1153): the complete state that decides the following steps (fields,
+ * potential, the four potential-increment buffers, the control block with the history times, dt lag, CFL rate
+ * and clock, and the statistics sums) copied to or from a caller-owned buffer of cavity_checkpoint_bytes
+ * bytes, on the device (fast snapshots: *_is_device = 1) or on the host (persistence).  Continuing from a
+ * loaded checkpoint is bit-identical to never having stopped.  A checkpoint loads only into a solver of the
+ * same grid size and precision form; both calls require no queued steps. */
+long long cavity_checkpoint_bytes(const CavitySolver* s);
+int cavity_checkpoint_save(CavitySolver* s, void* dst, int dst_is_device);
+int cavity_checkpoint_load(CavitySolver* s, const void* src, int src_is_device);
 /* Batches (no counterpart in the reference): cavities of the same grid size and precision form stepped
  * together by one CUDA graph per step, each of whose kernel launches covers every cavity.  Every cavity keeps
  * its own dt, pass count, clock and errors, and stays usable through its own handle between steps.  The

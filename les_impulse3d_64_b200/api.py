@@ -267,6 +267,21 @@ class Cavity:
         self._call('cavity_get_field', self.handle, FIELD_NUMBER[name], pointer(out))
         return out
 
+    def set_field(self, name, values):
+        dtype = np.float64 if name == 'phi' else np.float32
+        a = np.ascontiguousarray(values, dtype=dtype).reshape(self.shapes[name])
+        self._call('cavity_set_field', self.handle, FIELD_NUMBER[name], pointer(a))
+
+    def report(self):
+        r = Report()
+        self.lib.cavity_report.argtypes = [ct.c_void_p, ct.c_void_p]
+        self._call('cavity_report', self.handle, ct.byref(r))
+        return Solver._as_dict(r)
+
+    def set_clock(self, time, steps, last_dt):
+        self.lib.cavity_set_clock.argtypes = [ct.c_void_p, ct.c_double, ct.c_longlong, ct.c_double]
+        self._call('cavity_set_clock', self.handle, float(time), int(steps), float(last_dt))
+
     def probes(self):
         out = np.zeros(2 * self.config.n_probes, dtype=np.float32)
         self._call('cavity_probes', self.handle, pointer(out))
@@ -288,6 +303,32 @@ class Cavity:
         self._call('cavity_time_steps', self.handle, int(warmup), int(steps), int(bool(flush_l2)), pointer(ms),
                    pointer(kms))
         return ms, kms
+
+    def checkpoint(self, device_buffer=None):
+        """The complete state (fields, potential history, dt lag, clock, statistics): into a new host array, or
+        into `device_buffer` (a device pointer of at least `checkpoint_bytes()` bytes)."""
+        L = self.lib
+        L.cavity_checkpoint_save.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int]
+        if device_buffer is not None:
+            self._call('cavity_checkpoint_save', self.handle, ct.c_void_p(device_buffer), 1)
+            return device_buffer
+        out = np.empty(self.checkpoint_bytes(), dtype=np.uint8)
+        self._call('cavity_checkpoint_save', self.handle, out.ctypes.data_as(ct.c_void_p), 0)
+        return out
+
+    def restore(self, checkpoint):
+        """Load a state saved by `checkpoint` (a host array, or an int device pointer)."""
+        L = self.lib
+        L.cavity_checkpoint_load.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int]
+        if isinstance(checkpoint, np.ndarray):
+            self._call('cavity_checkpoint_load', self.handle, checkpoint.ctypes.data_as(ct.c_void_p), 0)
+        else:
+            self._call('cavity_checkpoint_load', self.handle, ct.c_void_p(checkpoint), 1)
+
+    def checkpoint_bytes(self):
+        self.lib.cavity_checkpoint_bytes.argtypes = [ct.c_void_p]
+        self.lib.cavity_checkpoint_bytes.restype = ct.c_longlong
+        return int(self.lib.cavity_checkpoint_bytes(self.handle))
 
     def close(self):
         if self.handle:

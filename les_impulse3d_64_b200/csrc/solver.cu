@@ -100,6 +100,9 @@ public:
     virtual void probes(float* out) = 0;
     virtual void add_statistics(double weight, double* centreline) = 0;
     virtual void get_statistics(double* sums) = 0;
+    virtual long long checkpoint_bytes() const = 0;
+    virtual void checkpoint_save(void* dst, int device) = 0;
+    virtual void checkpoint_load(const void* src, int device) = 0;
     virtual void set_statistics(const double* sums) = 0;
     virtual void midplane(float* out) = 0;
     virtual void q_volume(int colour_w, float* q, float* colour) = 0;
@@ -323,6 +326,73 @@ public:
         update_cfl();
         check(cudaStreamSynchronize(stream_));
         pull_control();
+    }
+    // ---- checkpoints: the whole state that decides the following steps, including what the reference drops
+    // on restart (backend.cu:1153): the potential-increment history and its times, the dt lag and the CFL rate
+    // (all in the control block), plus the statistics sums.  Layout: header, control block, u, m, phi, the
+    // four history buffers, statistics; each part 256-byte aligned.
+    struct CkHeader {
+        unsigned long long magic;
+        int nx, ny, nz, field_bytes;
+    };
+    static constexpr unsigned long long kCkMagic = 0x43415654594b5031ull;
+    struct CkLayout {
+        size_t ctrl, u[3], m[3], phi, hist[4], stats, total;
+    };
+    CkLayout ck_layout() const {
+        CkLayout L;
+        size_t o = 256;
+        auto take = [&](size_t bytes) { const size_t at = o; o += (bytes + 255) / 256 * 256; return at; };
+        L.ctrl = take(sizeof(Control));
+        for (int k = 0; k < 3; k++) L.u[k] = take(sizeof(T) * size_[k]);
+        for (int k = 0; k < 3; k++) L.m[k] = take(sizeof(T) * size_[k]);
+        L.phi = take(sizeof(double) * n_cell_);
+        for (int k = 0; k < 4; k++) L.hist[k] = take(sizeof(double) * n_cell_);
+        L.stats = take(sizeof(double) * 6 * nx_ * ny_);
+        L.total = o;
+        return L;
+    }
+    long long checkpoint_bytes() const override { return (long long)ck_layout().total; }
+    void checkpoint_save(void* dst, int device) override {
+        if (!pending_.empty()) fail("checkpoint: steps are queued; sync first");
+        const CkLayout L = ck_layout();
+        const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        char* d = static_cast<char*>(dst);
+        const CkHeader h{kCkMagic, nx_, ny_, nz_, (int)sizeof(T)};
+        check(cudaMemcpyAsync(d, &h, sizeof h, device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost, stream_));
+        check(cudaMemcpyAsync(d + L.ctrl, ctrl_, sizeof(Control), kind, stream_));
+        for (int k = 0; k < 3; k++) {
+            check(cudaMemcpyAsync(d + L.u[k], U_[par_][k], sizeof(T) * size_[k], kind, stream_));
+            check(cudaMemcpyAsync(d + L.m[k], M_[par_][k], sizeof(T) * size_[k], kind, stream_));
+        }
+        check(cudaMemcpyAsync(d + L.phi, PHI_[par_], sizeof(double) * n_cell_, kind, stream_));
+        for (int k = 0; k < 4; k++) check(cudaMemcpyAsync(d + L.hist[k], hist_[k], sizeof(double) * n_cell_, kind, stream_));
+        check(cudaMemcpyAsync(d + L.stats, stats_, sizeof(double) * 6 * nx_ * ny_, kind, stream_));
+        check(cudaStreamSynchronize(stream_));
+    }
+    void checkpoint_load(const void* src, int device) override {
+        if (!pending_.empty()) fail("checkpoint: steps are queued; sync first");
+        const CkLayout L = ck_layout();
+        const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        const char* d = static_cast<const char*>(src);
+        CkHeader h;
+        check(cudaMemcpy(&h, d, sizeof h, device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+        if (h.magic != kCkMagic) fail("checkpoint: not a cavity checkpoint");
+        if (h.nx != nx_ || h.ny != ny_ || h.nz != nz_ || h.field_bytes != (int)sizeof(T))
+            fail("checkpoint: grid size or precision form differs from this solver");
+        check(cudaMemcpyAsync(ctrl_, d + L.ctrl, sizeof(Control), kind, stream_));
+        for (int k = 0; k < 3; k++) {
+            check(cudaMemcpyAsync(U_[par_][k], d + L.u[k], sizeof(T) * size_[k], kind, stream_));
+            check(cudaMemcpyAsync(M_[par_][k], d + L.m[k], sizeof(T) * size_[k], kind, stream_));
+        }
+        check(cudaMemcpyAsync(PHI_[par_], d + L.phi, sizeof(double) * n_cell_, kind, stream_));
+        for (int k = 0; k < 4; k++) check(cudaMemcpyAsync(hist_[k], d + L.hist[k], sizeof(double) * n_cell_, kind, stream_));
+        check(cudaMemcpyAsync(stats_, d + L.stats, sizeof(double) * 6 * nx_ * ny_, kind, stream_));
+        check(cudaStreamSynchronize(stream_));
+        pull_control();
+        hc_.error = kOk;
+        push_control();
+        check(cudaStreamSynchronize(stream_));
     }
     void set_clock(double t, long long steps, double last_dt) override {
         hc_.t = t; hc_.steps = steps; hc_.last_dt = last_dt;
@@ -1311,6 +1381,10 @@ int cavity_step(CavitySolver* s, CavityReport* r) { return safely([&] { H(s).ste
 int cavity_step_async(CavitySolver* s, int count) { return safely([&] { H(s).step_async(count); }); }
 int cavity_sync(CavitySolver* s, CavityReport* r) { return safely([&] { H(s).sync(r); }); }
 int cavity_get_field(CavitySolver* s, int field, void* out) { return safely([&] { H(s).get_field(field, out); }); }
+int cavity_report(CavitySolver* s, CavityReport* r) { return safely([&] { H(s).report(r); }); }
+int cavity_set_clock(CavitySolver* s, double t, long long steps, double last_dt) {
+    return safely([&] { H(s).set_clock(t, steps, last_dt); });
+}
 int cavity_set_field(CavitySolver* s, int field, const void* in) { return safely([&] { H(s).set_field(field, in); }); }
 int cavity_probes(CavitySolver* s, float* out) { return safely([&] { H(s).probes(out); }); }
 int cavity_diagnostics(CavitySolver* s, CavityDiagnostics* d) { return safely([&] { H(s).diagnostics(d); }); }
@@ -1322,6 +1396,19 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
     return safely([&] { H(s).time_steps(warmup, steps, flush_l2, ms, kms); });
 }
 CavitySolver* cavity_default(void) { return g_default; }
+long long cavity_checkpoint_bytes(const CavitySolver* s) { return s && s->s ? s->s->checkpoint_bytes() : -1; }
+int cavity_checkpoint_save(CavitySolver* s, void* dst, int dst_is_device) {
+    return safely([&] {
+        if (!dst) cavity::fail("checkpoint: null buffer");
+        H(s).checkpoint_save(dst, dst_is_device);
+    });
+}
+int cavity_checkpoint_load(CavitySolver* s, const void* src, int src_is_device) {
+    return safely([&] {
+        if (!src) cavity::fail("checkpoint: null buffer");
+        H(s).checkpoint_load(src, src_is_device);
+    });
+}
 int cavity_kernels_per_step(const CavitySolver* s, int passes) { return s && s->s ? s->s->kernels_per_step(passes) : -1; }
 int cavity_fdm_pass(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                     const double* inv_lambda, const double* r, double* phi, void* stream) {
