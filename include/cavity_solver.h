@@ -85,6 +85,9 @@ int cavity_set_field(CavitySolver* s, int field, const void* in);
 int cavity_report(CavitySolver* s, CavityReport* r);
 int cavity_set_clock(CavitySolver* s, double t, long long steps, double last_dt);
 int cavity_probes(CavitySolver* s, float* out);
+/* Handle forms of solver_add_statistics and solver_get_statistics (backend.cu:1168-1180). */
+int cavity_add_statistics(CavitySolver* s, double weight, double* centreline);
+int cavity_get_statistics(CavitySolver* s, double* sums);
 int cavity_diagnostics(CavitySolver* s, CavityDiagnostics* d);
 /* Device bytes this cavity holds (state, work arrays, pressure tables), for admission control. */
 long long cavity_device_bytes(const CavitySolver* s);
@@ -100,6 +103,14 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 CavitySolver* cavity_default(void);
 /* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */
 int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
+/* Queued steps with per-step outputs (no counterpart in the reference, whose run script makes a blocking
+ * round trip per step for solver_probes and solver_add_statistics): queue `count` steps, each followed on the
+ * device by its probe values (into a library-owned ring of pinned host memory, at most 4096 steps between
+ * syncs) and, if `statistics`, by the mid-span statistics weighted with that step's dt.  cavity_sync_outputs
+ * waits, fills the report, copies the probe values of up to max_steps queued steps (2*n_probes floats each,
+ * in order) and stores their number in *steps_out. */
+int cavity_step_outputs_async(CavitySolver* s, int count, int statistics);
+int cavity_sync_outputs(CavitySolver* s, CavityReport* r, float* probes, int max_steps, int* steps_out);
 /* Checkpoints (no counterpart in the reference, whose restart through solver_set_field drops the potential
  * history and the dt lag, backend.cu:1153): the complete state that decides the following steps (fields,
  * potential, the four potential-increment buffers, the control block with the history times, dt lag, CFL rate

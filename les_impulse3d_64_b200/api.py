@@ -304,6 +304,35 @@ class Cavity:
                    pointer(kms))
         return ms, kms
 
+    def step_outputs_async(self, count=1, statistics=False):
+        """Queue `count` steps, each followed on the device by its probe values and, if `statistics`, by the
+        mid-span statistics weighted with that step's dt."""
+        self.lib.cavity_step_outputs_async.argtypes = [ct.c_void_p, ct.c_int, ct.c_int]
+        self._call('cavity_step_outputs_async', self.handle, int(count), int(bool(statistics)))
+
+    def sync_outputs(self, max_steps=4096):
+        """Wait for the queued steps; (report, probe values of each queued step as [steps, 2 * n_probes])."""
+        L = self.lib
+        L.cavity_sync_outputs.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]
+        r = Report()
+        out = np.zeros((max_steps, 2 * self.config.n_probes), dtype=np.float32)
+        n = ct.c_int(0)
+        self._call('cavity_sync_outputs', self.handle, ct.byref(r), out.ctypes.data_as(ct.c_void_p), int(max_steps),
+                   ct.byref(n))
+        return Solver._as_dict(r), out[:n.value]
+
+    def statistics(self):
+        out = np.empty(6 * self.nx * self.ny, dtype=np.float64)
+        self.lib.cavity_get_statistics.argtypes = [ct.c_void_p, ct.c_void_p]
+        self._call('cavity_get_statistics', self.handle, out.ctypes.data_as(ct.c_void_p))
+        return out
+
+    def add_statistics(self, weight):
+        line = np.empty(5 * self.nx, dtype=np.float64)
+        self.lib.cavity_add_statistics.argtypes = [ct.c_void_p, ct.c_double, ct.c_void_p]
+        self._call('cavity_add_statistics', self.handle, float(weight), line.ctypes.data_as(ct.c_void_p))
+        return line
+
     def checkpoint(self, device_buffer=None):
         """The complete state (fields, potential history, dt lag, clock, statistics): into a new host array, or
         into `device_buffer` (a device pointer of at least `checkpoint_bytes()` bytes)."""

@@ -178,9 +178,15 @@ __global__ void probes_kernel(OutArgs<T> a, const int* cells, int n, float* out)
 __device__ __forceinline__ void midspan_layers(int nz, int& k1, int& k2) { k2 = nz / 2; k1 = (nz % 2) ? k2 : k2 - 1; }
 
 // weighted running sums of u, v, uu, vv, ww, uv on the mid-span plane (backend.cu:507-517) and the
-// centreline sample (backend.cu:519-532); threads [0, nx*ny) do the sums, the next nx the centreline
+// centreline sample (backend.cu:519-532); threads [0, nx*ny) do the sums, the next nx the centreline.  With a
+// control block `wc` the weight is the dt of the step just taken, read on the device (queued outputs), and a
+// failed step adds nothing.
 template <class T>
-__global__ void statistics_kernel(OutArgs<T> a, double weight, double* sums, double* centreline) {
+__global__ void statistics_kernel(OutArgs<T> a, double weight, const Control* wc, double* sums, double* centreline) {
+    if (wc) {
+        if (wc->error) return;
+        weight = wc->last_dt;
+    }
     const Params& p = a.p;
     const int t = blockIdx.x * kThreads + threadIdx.x;
     const int n = p.nx * p.ny;

@@ -100,6 +100,8 @@ public:
     virtual void probes(float* out) = 0;
     virtual void add_statistics(double weight, double* centreline) = 0;
     virtual void get_statistics(double* sums) = 0;
+    virtual void step_outputs_async(int count, int statistics) = 0;
+    virtual int sync_outputs(CavityReport* r, float* probes, int max_steps) = 0;
     virtual long long checkpoint_bytes() const = 0;
     virtual void checkpoint_save(void* dst, int device) = 0;
     virtual void checkpoint_load(const void* src, int device) = 0;
@@ -169,6 +171,7 @@ public:
         if (stream_) cudaStreamSynchronize(stream_);
         arena_.release();
         if (flush_) cudaFree(flush_);
+        if (ring_host_) cudaFreeHost(ring_host_);
         if (stream_) cudaStreamDestroy(stream_);
         if (body_stream_) cudaStreamDestroy(body_stream_);
     }
@@ -327,6 +330,43 @@ public:
         check(cudaStreamSynchronize(stream_));
         pull_control();
     }
+    // ---- queued steps with their per-step outputs on the device: after each step the probe values go into a
+    // ring of pinned, mapped host memory (written by the probe kernel, no copy), and optionally the mid-span
+    // statistics accumulate with that step's dt (backend.cu:507-517); nothing waits for the host until
+    // sync_outputs.  The reference's run script instead calls solver_step, solver_probes and
+    // solver_add_statistics per step, each a blocking round trip.
+    static constexpr int kRingSteps = 4096;
+    void step_outputs_async(int count, int statistics) override {
+        ensure_graphs(false);
+        const int np = c_.n_probes;
+        if (np > 0 && !ring_host_) {
+            check(cudaHostAlloc((void**)&ring_host_, sizeof(float) * 2 * np * kRingSteps, cudaHostAllocMapped));
+            check(cudaHostGetDevicePointer((void**)&ring_dev_, ring_host_, 0));
+        }
+        if (ring_n_ + count > kRingSteps) fail("queued outputs: at most 4096 steps between syncs");
+        for (int i = 0; i < count; i++) {
+            step_async(1);
+            if (np > 0) {
+                probes_kernel<T><<<1, 32, 0, stream_>>>(out_args(), probe_cells_, np, ring_dev_ + (size_t)ring_n_ * 2 * np);
+                ring_n_++;
+            }
+            if (statistics)
+                statistics_kernel<T><<<blocks_for((long long)nx_ * ny_ + nx_), kThreads, 0, stream_>>>(out_args(), 0.0, ctrl_,
+                                                                                                   stats_, line_);
+        }
+        check(cudaGetLastError());
+    }
+    // waits for the queued steps; copies the probe values of up to max_steps of them (2 n_probes floats each,
+    // in order) and returns how many steps they cover
+    int sync_outputs(CavityReport* r, float* probes, int max_steps) override {
+        const int queued = ring_n_;
+        ring_n_ = 0;
+        sync(r);
+        const int n = std::min(queued, std::max(max_steps, 0));
+        if (n > 0 && probes) std::memcpy(probes, ring_host_, sizeof(float) * 2 * c_.n_probes * n);
+        return n;
+    }
+
     // ---- checkpoints: the whole state that decides the following steps, including what the reference drops
     // on restart (backend.cu:1153): the potential-increment history and its times, the dt lag and the CFL rate
     // (all in the control block), plus the statistics sums.  Layout: header, control block, u, m, phi, the
@@ -406,7 +446,7 @@ public:
         check(cudaStreamSynchronize(stream_));
     }
     void add_statistics(double weight, double* centreline) override {                  // backend.cu:1168-1175
-        statistics_kernel<T><<<blocks_for((long long)nx_ * ny_ + nx_), kThreads, 0, stream_>>>(out_args(), weight, stats_, line_);
+        statistics_kernel<T><<<blocks_for((long long)nx_ * ny_ + nx_), kThreads, 0, stream_>>>(out_args(), weight, nullptr, stats_, line_);
         check(cudaMemcpyAsync(centreline, line_, sizeof(double) * 5 * nx_, cudaMemcpyDeviceToHost, stream_));
         check(cudaStreamSynchronize(stream_));
     }
@@ -926,6 +966,9 @@ private:
     cudaGraphExec_t exec_[2] = {nullptr, nullptr}, texec_[2] = {nullptr, nullptr};
     cudaEvent_t kev_[6] = {};
     void* flush_ = nullptr;
+    float* ring_host_ = nullptr;       // queued per-step probe values (pinned, mapped)
+    float* ring_dev_ = nullptr;
+    int ring_n_ = 0;
 };
 
 
@@ -1387,6 +1430,10 @@ int cavity_set_clock(CavitySolver* s, double t, long long steps, double last_dt)
 }
 int cavity_set_field(CavitySolver* s, int field, const void* in) { return safely([&] { H(s).set_field(field, in); }); }
 int cavity_probes(CavitySolver* s, float* out) { return safely([&] { H(s).probes(out); }); }
+int cavity_add_statistics(CavitySolver* s, double weight, double* centreline) {
+    return safely([&] { H(s).add_statistics(weight, centreline); });
+}
+int cavity_get_statistics(CavitySolver* s, double* sums) { return safely([&] { H(s).get_statistics(sums); }); }
 int cavity_diagnostics(CavitySolver* s, CavityDiagnostics* d) { return safely([&] { H(s).diagnostics(d); }); }
 long long cavity_device_bytes(const CavitySolver* s) { return s && s->s ? s->s->device_bytes() : -1; }
 long long cavity_estimate_bytes(const CavityConfig* config, int precision) {
@@ -1396,6 +1443,15 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
     return safely([&] { H(s).time_steps(warmup, steps, flush_l2, ms, kms); });
 }
 CavitySolver* cavity_default(void) { return g_default; }
+int cavity_step_outputs_async(CavitySolver* s, int count, int statistics) {
+    return safely([&] { H(s).step_outputs_async(count, statistics); });
+}
+int cavity_sync_outputs(CavitySolver* s, CavityReport* r, float* probes, int max_steps, int* steps_out) {
+    return safely([&] {
+        const int n = H(s).sync_outputs(r, probes, max_steps);
+        if (steps_out) *steps_out = n;
+    });
+}
 long long cavity_checkpoint_bytes(const CavitySolver* s) { return s && s->s ? s->s->checkpoint_bytes() : -1; }
 int cavity_checkpoint_save(CavitySolver* s, void* dst, int dst_is_device) {
     return safely([&] {
