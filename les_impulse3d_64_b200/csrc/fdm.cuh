@@ -31,12 +31,16 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* src, int s
     const unsigned int dst = (unsigned int)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
 }
+__device__ __forceinline__ void cp_async16z(void* smem_dst, const void* src, int src_bytes) {
+    const unsigned int dst = (unsigned int)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // CTA tile BM x BN from WARPS_M x WARPS_N warps; K consumed in panels of KC with every load of a panel in
-// flight at once (cp.async, zero-filled outside the matrices).
+// flight at once (cp.async, zero-filled outside the matrices; two doubles per copy where rows allow).
 template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
 __device__ void dgemm_mma_body(const GemmArgs<double>& g, const Blk& blk, bool first) {
     pdl_launch_dependents();
@@ -45,8 +49,8 @@ __device__ void dgemm_mma_body(const GemmArgs<double>& g, const Blk& blk, bool f
     constexpr int WTM = BM / WARPS_M, WTN = BN / WARPS_N;     // warp tile
     constexpr int FM = WTM / 8, FN = WTN / 8;                   // fragments per warp tile
     constexpr int LDA = KC + 4, LDB = BN + 4;                   // row pitches of 8 banks mod 32
-    __shared__ double As[BM * LDA];
-    __shared__ double Bs[KC * LDB];
+    __shared__ __align__(16) double As[BM * LDA];
+    __shared__ __align__(16) double Bs[KC * LDB];
     if (g.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(g.handle, 0u);
     const Control* c = g.c;
     if (c->error || !c->cond) return;                     // failed, or this cavity's refinement has ended
@@ -59,21 +63,40 @@ __device__ void dgemm_mma_body(const GemmArgs<double>& g, const Blk& blk, bool f
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = warp / WARPS_N, wn = warp % WARPS_N;
     const int fr = lane >> 2, fc = lane & 3;          // fragment row / column of this lane
+    // two doubles per copy when rows are even and the arrays 16-byte aligned
+    const bool a2 = g.K % 2 == 0 && g.lda % 2 == 0 && ((unsigned long long)A & 15) == 0;
+    const bool b2 = g.N % 2 == 0 && g.ldb % 2 == 0 && ((unsigned long long)B & 15) == 0;
     double acc[FM][FN][2];
 #pragma unroll
     for (int i = 0; i < FM; i++)
 #pragma unroll
         for (int j = 0; j < FN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
     for (int k0 = 0; k0 < g.K; k0 += KC) {
-        for (int e = threadIdx.x; e < BM * KC; e += NT) {
-            const int r = e / KC, k = e % KC, gm = m0 + r, gk = k0 + k;
-            const bool ok = gm < g.M && gk < g.K;
-            cp_async8(&As[r * LDA + k], ok ? A + (long long)gm * g.lda + gk : A, ok ? 8 : 0);
+        if (a2) {
+            for (int e = threadIdx.x; e < BM * KC / 2; e += NT) {
+                const int r = e / (KC / 2), k = 2 * (e % (KC / 2)), gm = m0 + r, gk = k0 + k;
+                const bool ok = gm < g.M && gk < g.K;
+                cp_async16z(&As[r * LDA + k], ok ? A + (long long)gm * g.lda + gk : A, ok ? 16 : 0);
+            }
+        } else {
+            for (int e = threadIdx.x; e < BM * KC; e += NT) {
+                const int r = e / KC, k = e % KC, gm = m0 + r, gk = k0 + k;
+                const bool ok = gm < g.M && gk < g.K;
+                cp_async8(&As[r * LDA + k], ok ? A + (long long)gm * g.lda + gk : A, ok ? 8 : 0);
+            }
         }
-        for (int e = threadIdx.x; e < KC * BN; e += NT) {
-            const int k = e / BN, col = e % BN, gk = k0 + k, gn = n0 + col;
-            const bool ok = gk < g.K && gn < g.N;
-            cp_async8(&Bs[k * LDB + col], ok ? B + (long long)gk * g.ldb + gn : B, ok ? 8 : 0);
+        if (b2) {
+            for (int e = threadIdx.x; e < KC * BN / 2; e += NT) {
+                const int k = e / (BN / 2), col = 2 * (e % (BN / 2)), gk = k0 + k, gn = n0 + col;
+                const bool ok = gk < g.K && gn < g.N;
+                cp_async16z(&Bs[k * LDB + col], ok ? B + (long long)gk * g.ldb + gn : B, ok ? 16 : 0);
+            }
+        } else {
+            for (int e = threadIdx.x; e < KC * BN; e += NT) {
+                const int k = e / BN, col = e % BN, gk = k0 + k, gn = n0 + col;
+                const bool ok = gk < g.K && gn < g.N;
+                cp_async8(&Bs[k * LDB + col], ok ? B + (long long)gk * g.ldb + gn : B, ok ? 8 : 0);
+            }
         }
         cp_async_wait_all();
         __syncthreads();
