@@ -192,6 +192,25 @@ __device__ __forceinline__ Blk batch_blk(unsigned int per, int& cavity) {
     return {blockIdx.x, blockIdx.y, blockIdx.z % per, gridDim.x, gridDim.y, per};
 }
 __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0; }
+// Cells visited as columns: a block takes kThreads consecutive cells of an x-y plane (x fastest) and walks them
+// up a chunk of z-layers; grid y runs over the chunks.  A thread's plane position, and so its x and y table
+// values, stay fixed, and its column's values below and at the current layer carry over in registers.
+struct ColumnSpan {
+    int p, x, y, z0, z1;
+    bool live;
+};
+__device__ __forceinline__ ColumnSpan column_span(const Params& p, const Blk& k) {
+    ColumnSpan s;
+    const int plane = p.nx * p.ny;
+    s.p = (int)k.x * kThreads + (int)threadIdx.x;
+    s.live = s.p < plane;
+    s.x = s.p % p.nx;
+    s.y = s.p / p.nx;
+    const int zc = (p.nz + (int)k.ny - 1) / (int)k.ny;
+    s.z0 = (int)k.y * zc;
+    s.z1 = min(p.nz, s.z0 + zc);
+    return s;
+}
 // Programmatic dependent launch: the step kernels are launched so that the next kernel may start while this one
 // finishes.  Every step kernel lets its dependents launch at entry and waits for its predecessor to complete
 // (with all its memory visible) before it reads anything a predecessor wrote.  Both are no-ops for a kernel
@@ -509,7 +528,7 @@ __global__ void __launch_bounds__(kThreads) projection_start_batched(const Start
 
 // ------------------------------------------------------------------------------------------ residual
 // r = rhs - L phi with L the 7-point area-weighted Neumann Laplacian (backend.cu:345-359) after a pass, sum r^2
-// and sum phi; the last block counts the pass and decides on the next (backend.cu:835-839).  Grid-stride.
+// and sum phi; the last block counts the pass and decides on the next (backend.cu:835-839).  Column walk.
 struct ResidualArgs {
     Params p;
     const double* dw[3];
@@ -524,6 +543,7 @@ struct ResidualArgs {
 };
 
 // A cavity whose refinement loop has ended (a batch runs passes while any cavity needs one) skips the pass.
+// Column walk (ColumnSpan); each cell's arithmetic is that of backend.cu:352-357.
 __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     pdl_launch_dependents();
     pdl_wait();
@@ -534,24 +554,34 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     Vec<2> acc;
     acc.v[0] = 0.0;
     acc.v[1] = 0.0;
-    const int sy = p.nx, sz = p.nx * p.ny;
-    if (!err) {
-        for (int i = k.x * kThreads + threadIdx.x; i < p.n_cell; i += k.nx * kThreads) {
-            const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
-            const double dx = a.dw[X][x], dy = a.dw[Y][y], dz = a.dw[Z][z];
-            const double* f = a.phi;
-            const double cc = f[i];
+    const ColumnSpan cs = column_span(p, k);
+    if (!err && cs.live) {
+        const int sy = p.nx, sz = p.nx * p.ny, x = cs.x, y = cs.y;
+        const double dx = a.dw[X][x], dy = a.dw[Y][y];
+        const bool xl = x > 0, xh = x + 1 < p.nx, yl = y > 0, yh = y + 1 < p.ny;
+        const double ixl = a.dinv_sp[X][x], ixh = a.dinv_sp[X][x + 1], iyl = a.dinv_sp[Y][y], iyh = a.dinv_sp[Y][y + 1];
+        const double* f = a.phi;
+        int i = cs.p + cs.z0 * sz;
+        double below = cs.z0 > 0 && cs.z0 < cs.z1 ? __ldg(f + i - sz) : 0.0;
+        double cc = cs.z0 < cs.z1 ? __ldg(f + i) : 0.0;
+#pragma unroll 2
+        for (int z = cs.z0; z < cs.z1; z++, i += sz) {
+            const bool zh = z + 1 < p.nz;
+            const double above = zh ? __ldg(f + i + sz) : 0.0;
+            const double dz = a.dw[Z][z];
             double s = 0.0;
-            if (x + 1 < p.nx) s += (dy * dz) * (f[i + 1] - cc) * a.dinv_sp[X][x + 1];
-            if (x > 0) s -= (dy * dz) * (cc - f[i - 1]) * a.dinv_sp[X][x];
-            if (y + 1 < p.ny) s += (dx * dz) * (f[i + sy] - cc) * a.dinv_sp[Y][y + 1];
-            if (y > 0) s -= (dx * dz) * (cc - f[i - sy]) * a.dinv_sp[Y][y];
-            if (z + 1 < p.nz) s += (dx * dy) * (f[i + sz] - cc) * a.dinv_sp[Z][z + 1];
-            if (z > 0) s -= (dx * dy) * (cc - f[i - sz]) * a.dinv_sp[Z][z];
-            const double r = a.rhs[i] - s;
+            if (xh) s += (dy * dz) * (__ldg(f + i + 1) - cc) * ixh;
+            if (xl) s -= (dy * dz) * (cc - __ldg(f + i - 1)) * ixl;
+            if (yh) s += (dx * dz) * (__ldg(f + i + sy) - cc) * iyh;
+            if (yl) s -= (dx * dz) * (cc - __ldg(f + i - sy)) * iyl;
+            if (zh) s += (dx * dy) * (above - cc) * a.dinv_sp[Z][z + 1];
+            if (z > 0) s -= (dx * dy) * (cc - below) * a.dinv_sp[Z][z];
+            const double r = __ldg(a.rhs + i) - s;
             a.res[i] = r;
             acc.v[0] += r * r;
             acc.v[1] += cc;
+            below = cc;
+            cc = above;
         }
     }
     const Vec<2> blk = block_reduce<2, false>(acc);

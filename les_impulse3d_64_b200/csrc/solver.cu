@@ -543,7 +543,9 @@ private:
         t1_ = arena_.alloc<double>(n_cell_);
         t2_ = arena_.alloc<double>(n_cell_);
         inv_lambda_ = arena_.alloc<double>(n_cell_);
-        partial_blocks_ = (long long)blocks_for(std::max(max_face_, n_cell_)) + 8;
+        // the grid-stride kernels' blocks, or the column kernels' plane blocks x z-chunks (at most one chunk per layer)
+        partial_blocks_ = std::max((long long)blocks_for(std::max(max_face_, n_cell_)),
+                                   (long long)blocks_for((long long)nx_ * ny_) * nz_) + 8;
         int sms = 148, dev = 0;
         check(cudaGetDevice(&dev));
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -557,7 +559,7 @@ private:
             return (unsigned int)std::min<long long>(blocks_for(n_cell_), (long long)std::max(per_sm, 1) * sms);
         };
         start_blocks_ = resident((const void*)projection_start_kernel<T>);
-        residual_blocks_ = resident((const void*)residual_kernel);
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&residual_per_sm_, (const void*)residual_kernel, kThreads, 0));
         finish_blocks_ = resident((const void*)finish_kernel<T>);
         if (tc_fdm_) {
             inv_lambda_f_ = arena_.alloc<float>(n_cell_);
@@ -710,6 +712,17 @@ private:
     // grid of a recorded cell kernel: in a batch the launch already spans many cavities, so each cavity keeps
     // the smaller grid (fewer partials per reduction)
     unsigned int cell_grid(unsigned int alone) const { return g_launch_batch > 1 ? cell_blocks_ : alone; }
+    // grid of a column kernel (ColumnSpan): plane blocks along x and z-chunks along y, as many chunks as it takes
+    // for the launch (all cavities of a batch together) to fill the device `per_sm` blocks deep
+    dim3 column_grid(int per_sm) const {
+        const long long bpp = blocks_for((long long)nx_ * ny_);
+        const long long want = (long long)sms_ * std::max(per_sm, 1);
+        const long long cav = std::max(g_launch_batch, 1);
+        long long chunks = std::min<long long>(nz_, std::max(1LL, (want + bpp * cav - 1) / (bpp * cav)));
+        const long long zc = (nz_ + chunks - 1) / chunks;
+        chunks = (nz_ + zc - 1) / zc;
+        return dim3((unsigned int)bpp, (unsigned int)chunks);
+    }
     void launch_step_begin(cudaStream_t st) {
         StepBeginArgs a;
         a.p = p_;
@@ -778,8 +791,8 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        if (!record_launch(kLkResidual, 0, dim3(cell_grid(residual_blocks_)), 0, a))
-            check(launch_pdl(residual_kernel, dim3(residual_blocks_), dim3(kThreads), 0, st, a));
+        const dim3 grid = column_grid(residual_per_sm_);
+        if (!record_launch(kLkResidual, 0, grid, 0, a)) check(launch_pdl(residual_kernel, grid, dim3(kThreads), 0, st, a));
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
@@ -955,7 +968,8 @@ private:
     double* partial_;
     long long partial_blocks_;
     unsigned int cell_blocks_ = 1;     // grid of other grid-stride cell kernels: at most 4 CTAs per SM
-    unsigned int start_blocks_ = 1, residual_blocks_ = 1, finish_blocks_ = 1;
+    unsigned int start_blocks_ = 1, finish_blocks_ = 1;
+    int residual_per_sm_ = 1;
     Control* ctrl_;
     double *slots_, *stats_, *line_, *dstage_[2];
     unsigned int* out_counters_;
