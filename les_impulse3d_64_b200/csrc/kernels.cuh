@@ -339,14 +339,14 @@ template <class T> struct MomentumArgs {
 };
 
 // ------------------------------------------------------------------------------------------ start of a projection
-// rhs = volume * div(m) in FP64 (backend.cu:334-342) and the residual r = rhs - L guess of the starting potential
-// (backend.cu:825-829).  In a step the starting potential is the warm-start guess: the potential carried by
-// the RK combination (base, backend.cu:922-923) plus the extrapolated increments (backend.cu:924-925,
-// 857-873), evaluated here at each cell and its six neighbours; stage 0 also stores phi0 = r phi
-// (backend.cu:882).  A plain projection (initialize, kick) starts from zero.  The last block takes the
-// reference's start-of-solve decisions (backend.cu:818-831): NaN right-hand side (error), zero right-hand side
-// (phi = 0, no pass), a guess no better than zero (dropped: start from phi = 0 with r = rhs), and whether the
-// refinement loop runs.  Grid-stride over cells.
+// rhs = volume * div(m) in FP64 (backend.cu:334-342) and the starting potential of the solve.  In a step that is
+// the warm-start guess: the potential carried by the RK combination (base, backend.cu:922-923) plus the
+// extrapolated increments (backend.cu:924-925, 857-873); stage 0 also stores phi0 = r phi (backend.cu:882).
+// Its residual r = rhs - L guess (backend.cu:825-829) needs the guess of neighbouring cells, so the start mode
+// of the residual kernel computes it next and takes the decisions that depend on it.  A plain projection
+// (initialize, kick) starts from zero with r = rhs.  The last block takes the reference's start-of-solve
+// decisions (backend.cu:818-831) that need only the right-hand side: NaN (error), zero (phi = 0, no pass), and,
+// starting from zero, whether the refinement loop runs.  Column walk (ColumnSpan).
 template <class T> struct StartArgs {
     Params p;
     Geo<T> g;
@@ -432,53 +432,71 @@ __device__ void projection_start_body(const StartArgs<T>& a, const Blk& k) {
     int b1 = -1, b2 = -1;
     double c1 = 0, c2 = 0;
     if (have_guess) guess_coefficients(p, c, sc.tau, sc.b * c->dt, b1, c1, b2, c2);
-    // base and guess at cell j
-    auto base_at = [&](int j) {
-        return a.stage == 0 ? sc.b * (p.reinit_r * a.phi_state[j]) : sc.a0 * a.phi0[j] + sc.b * a.phi_cur[j];
-    };
-    auto guess_from = [&](double base, int j) {
-        if (b1 < 0) return base;
-        const double ex = b2 >= 0 ? c1 * a.hist[b1][j] + c2 * a.hist[b2][j] : c1 * a.hist[b1][j];
-        return ex + base;
-    };
-    auto guess_at = [&](int j) { return guess_from(base_at(j), j); };
-    Vec<3> acc;
-    acc.v[0] = acc.v[1] = acc.v[2] = 0.0;
-    const int sy = p.nx, sz = p.nx * p.ny;
-    if (!err) {
-        for (int i = k.x * kThreads + threadIdx.x; i < p.n_cell; i += k.nx * kThreads) {
-            const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
-            const double dx = a.g.dw[X][x], dy = a.g.dw[Y][y], dz = a.g.dw[Z][z];
-            const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
-            const double rhs = ((double)a.m[X][iu + 1] - (double)a.m[X][iu]) * (dy * dz) +
-                               ((double)a.m[Y][iv + p.nx] - (double)a.m[Y][iv]) * (dx * dz) +
-                               ((double)a.m[Z][iw + p.nx * p.ny] - (double)a.m[Z][iw]) * (dx * dy);
+    Vec<1> acc;
+    acc.v[0] = 0.0;
+    const ColumnSpan cs = column_span(p, k);
+    if (!err && cs.live && cs.z0 < cs.z1) {
+        const int x = cs.x, y = cs.y, nx = p.nx, sz = p.nx * p.ny;
+        const int su = (p.nx + 1) * p.ny, sv = p.nx * (p.ny + 1);     // layer strides of the u and v faces
+        const double dx = a.g.dw[X][x], dy = a.g.dw[Y][y];
+        // the loads of a layer, issued one layer ahead of its arithmetic
+        struct Layer { T mx0, mx1, my0, my1, mz1; double dz, ph, p0, h1, h2; };
+        auto fetch = [&](int j, int ju, int jv, int z) {
+            Layer v;
+            v.mx0 = __ldg(a.m[X] + ju);
+            v.mx1 = __ldg(a.m[X] + ju + 1);
+            v.my0 = __ldg(a.m[Y] + jv);
+            v.my1 = __ldg(a.m[Y] + jv + nx);
+            v.mz1 = __ldg(a.m[Z] + j + sz);
+            v.dz = __ldg(a.g.dw[Z] + z);
+            v.ph = v.p0 = v.h1 = v.h2 = 0.0;
+            if (have_guess) {
+                if (a.stage == 0) v.ph = __ldg(a.phi_state + j);
+                else { v.p0 = __ldg(a.phi0 + j); v.ph = __ldg(a.phi_cur + j); }
+                if (b1 >= 0) v.h1 = __ldg(a.hist[b1] + j);
+                if (b2 >= 0) v.h2 = __ldg(a.hist[b2] + j);
+            }
+            return v;
+        };
+        int i = cs.p + cs.z0 * sz;
+        int iu = fidx<X>(p, x, y, cs.z0), iv = fidx<Y>(p, x, y, cs.z0);
+        T wlo = __ldg(a.m[Z] + i);                                     // m_z on this cell's lower face
+        Layer next = fetch(i, iu, iv, cs.z0);
+        for (int z = cs.z0; z < cs.z1; z++, i += sz, iu += su, iv += sv) {
+            const Layer l = next;
+            if (z + 1 < cs.z1) next = fetch(i + sz, iu + su, iv + sv, z + 1);
+            const double dz = l.dz;
+            const double rhs = ((double)l.mx1 - (double)l.mx0) * (dy * dz) + ((double)l.my1 - (double)l.my0) * (dx * dz) +
+                               ((double)l.mz1 - (double)wlo) * (dx * dy);
+            wlo = l.mz1;
             a.rhs[i] = rhs;
             acc.v[0] += rhs * rhs;
-            double r = rhs, g = 0.0;
             if (have_guess) {
-                const double base = base_at(i);
-                if (a.stage == 0) a.phi0[i] = p.reinit_r * a.phi_state[i];
+                // base and guess (backend.cu:922-928, 857-873); their residual is the start mode of the
+                // residual kernel, which reads the guess of the neighbouring cells
+                double base;
+                if (a.stage == 0) {
+                    base = sc.b * (p.reinit_r * l.ph);
+                    a.phi0[i] = p.reinit_r * l.ph;
+                } else {
+                    base = sc.a0 * l.p0 + sc.b * l.ph;
+                }
                 a.base[i] = base;
-                g = guess_from(base, i);
-                double s = 0.0;           // L g, backend.cu:352-357
-                if (x + 1 < p.nx) s += (dy * dz) * (guess_at(i + 1) - g) * a.g.dinv_sp[X][x + 1];
-                if (x > 0) s -= (dy * dz) * (g - guess_at(i - 1)) * a.g.dinv_sp[X][x];
-                if (y + 1 < p.ny) s += (dx * dz) * (guess_at(i + sy) - g) * a.g.dinv_sp[Y][y + 1];
-                if (y > 0) s -= (dx * dz) * (g - guess_at(i - sy)) * a.g.dinv_sp[Y][y];
-                if (z + 1 < p.nz) s += (dx * dy) * (guess_at(i + sz) - g) * a.g.dinv_sp[Z][z + 1];
-                if (z > 0) s -= (dx * dy) * (g - guess_at(i - sz)) * a.g.dinv_sp[Z][z];
-                r = rhs - s;
+                double g = base;
+                if (b1 >= 0) {
+                    const double ex = b2 >= 0 ? c1 * l.h1 + c2 * l.h2 : c1 * l.h1;
+                    g = ex + base;
+                }
+                a.guess[i] = g;
+            } else {
+                a.guess[i] = 0.0;
+                a.res[i] = rhs;
             }
-            a.guess[i] = g;
-            a.res[i] = r;
-            acc.v[1] += r * r;
-            acc.v[2] += g;
         }
     }
-    const Vec<3> blk = block_reduce<3, false>(acc);
+    const Vec<1> blk = block_reduce<1, false>(acc);
     if (publish_partials(blk, a.partial, &c->counter[kCntDiv], k)) {
-        const Vec<3> tot = final_reduce<3, false>(a.partial, k);
+        const Vec<1> tot = final_reduce<1, false>(a.partial, k);
         if (threadIdx.x == 0) {
             c->counter[kCntDiv] = 0;
             c->passes = 0;
@@ -498,18 +516,12 @@ __device__ void projection_start_body(const StartArgs<T>& a, const Blk& k) {
                 set_loop(c, a.handle, a.use_handle, 0);
                 return;
             }
-            double rel = 1.0;
-            c->use_rhs = 1;
-            c->phi_sum = 0.0;
-            if (have_guess) {
-                rel = sqrt(tot.v[1]) / c->rhs_norm;
-                c->res_norm2 = tot.v[1];
-                c->use_rhs = 0;
-                c->phi_sum = tot.v[2];
-                if (rel >= 1.0) { rel = 1.0; c->use_rhs = 1; c->reset_phi = 1; c->phi_sum = 0.0; }
+            if (!have_guess) {                                // start from phi = 0: the residual is rhs
+                c->use_rhs = 1;
+                c->phi_sum = 0.0;
+                c->rel = 1.0;
+                decide_loop(p, c, a.handle, a.use_handle);
             }
-            c->rel = rel;
-            decide_loop(p, c, a.handle, a.use_handle);
         }
     }
 }
@@ -540,6 +552,7 @@ struct ResidualArgs {
     double* partial;
     cudaGraphConditionalHandle handle;
     int use_handle;
+    int start;                 // 1: residual of the warm-start guess at the start of a solve (phi = the guess)
 };
 
 // A cavity whose refinement loop has ended (a batch runs passes while any cavity needs one) skips the pass.
@@ -548,40 +561,56 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     pdl_launch_dependents();
     pdl_wait();
     Control* c = a.c;
-    if (!c->cond) return;
+    if (!a.start && !c->cond) return;
     const Params& p = a.p;
     const int err = c->error;
+    const bool skip = err || (a.start && c->zero_rhs);
     Vec<2> acc;
     acc.v[0] = 0.0;
     acc.v[1] = 0.0;
     const ColumnSpan cs = column_span(p, k);
-    if (!err && cs.live) {
+    if (!skip && cs.live && cs.z0 < cs.z1) {
         const int sy = p.nx, sz = p.nx * p.ny, x = cs.x, y = cs.y;
         const double dx = a.dw[X][x], dy = a.dw[Y][y];
         const bool xl = x > 0, xh = x + 1 < p.nx, yl = y > 0, yh = y + 1 < p.ny;
         const double ixl = a.dinv_sp[X][x], ixh = a.dinv_sp[X][x + 1], iyl = a.dinv_sp[Y][y], iyh = a.dinv_sp[Y][y + 1];
         const double* f = a.phi;
+        // the loads of a layer, issued one layer ahead of its arithmetic
+        struct Layer { double above, e, w, n, s, rhs, dz, izl, izh; };
+        auto fetch = [&](int j, int z) {
+            Layer v;
+            v.above = z + 1 < p.nz ? __ldg(f + j + sz) : 0.0;
+            v.e = xh ? __ldg(f + j + 1) : 0.0;
+            v.w = xl ? __ldg(f + j - 1) : 0.0;
+            v.n = yh ? __ldg(f + j + sy) : 0.0;
+            v.s = yl ? __ldg(f + j - sy) : 0.0;
+            v.rhs = __ldg(a.rhs + j);
+            v.dz = __ldg(a.dw[Z] + z);
+            v.izl = __ldg(a.dinv_sp[Z] + z);
+            v.izh = __ldg(a.dinv_sp[Z] + z + 1);
+            return v;
+        };
         int i = cs.p + cs.z0 * sz;
-        double below = cs.z0 > 0 && cs.z0 < cs.z1 ? __ldg(f + i - sz) : 0.0;
-        double cc = cs.z0 < cs.z1 ? __ldg(f + i) : 0.0;
-#pragma unroll 2
+        double below = cs.z0 > 0 ? __ldg(f + i - sz) : 0.0;
+        double cc = __ldg(f + i);
+        Layer next = fetch(i, cs.z0);
         for (int z = cs.z0; z < cs.z1; z++, i += sz) {
-            const bool zh = z + 1 < p.nz;
-            const double above = zh ? __ldg(f + i + sz) : 0.0;
-            const double dz = a.dw[Z][z];
+            const Layer l = next;
+            if (z + 1 < cs.z1) next = fetch(i + sz, z + 1);
+            const double dz = l.dz;
             double s = 0.0;
-            if (xh) s += (dy * dz) * (__ldg(f + i + 1) - cc) * ixh;
-            if (xl) s -= (dy * dz) * (cc - __ldg(f + i - 1)) * ixl;
-            if (yh) s += (dx * dz) * (__ldg(f + i + sy) - cc) * iyh;
-            if (yl) s -= (dx * dz) * (cc - __ldg(f + i - sy)) * iyl;
-            if (zh) s += (dx * dy) * (above - cc) * a.dinv_sp[Z][z + 1];
-            if (z > 0) s -= (dx * dy) * (cc - below) * a.dinv_sp[Z][z];
-            const double r = __ldg(a.rhs + i) - s;
+            if (xh) s += (dy * dz) * (l.e - cc) * ixh;
+            if (xl) s -= (dy * dz) * (cc - l.w) * ixl;
+            if (yh) s += (dx * dz) * (l.n - cc) * iyh;
+            if (yl) s -= (dx * dz) * (cc - l.s) * iyl;
+            if (z + 1 < p.nz) s += (dx * dy) * (l.above - cc) * l.izh;
+            if (z > 0) s -= (dx * dy) * (cc - below) * l.izl;
+            const double r = l.rhs - s;
             a.res[i] = r;
             acc.v[0] += r * r;
             acc.v[1] += cc;
             below = cc;
-            cc = above;
+            cc = l.above;
         }
     }
     const Vec<2> blk = block_reduce<2, false>(acc);
@@ -590,6 +619,19 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
         if (threadIdx.x == 0) {
             c->counter[kCntRes] = 0;
             if (err) { set_loop(c, a.handle, a.use_handle, 0); return; }
+            if (a.start) {
+                // the guess is kept unless it is no better than zero (backend.cu:825-831); a zero right-hand
+                // side was decided with it
+                if (c->zero_rhs) return;
+                double rel = sqrt(tot.v[0]) / c->rhs_norm;
+                c->res_norm2 = tot.v[0];
+                c->use_rhs = 0;
+                c->phi_sum = tot.v[1];
+                if (rel >= 1.0) { rel = 1.0; c->use_rhs = 1; c->reset_phi = 1; c->phi_sum = 0.0; }
+                c->rel = rel;
+                decide_loop(p, c, a.handle, a.use_handle);
+                return;
+            }
             c->passes += 1;
             c->phi_passes = c->passes;
             c->pass_count += 1;
@@ -639,8 +681,8 @@ template <class D> struct GemmArgs {
 // ------------------------------------------------------------------------------------------ finish a projection
 // u = m - grad(phi) with phi's mean removed (backend.cu:846, 361-371); the potential increment history
 // (backend.cu:929-939); in the last stage the CFL rate of the new velocity for the next step's dt
-// (backend.cu:465-472) and the clock update (backend.cu:945-954).  One thread per cell; the thread of the
-// last cell along an axis also writes the wall face beyond it.  The solution is read from one buffer and the
+// (backend.cu:465-472) and the clock update (backend.cu:945-954).  Column walk (ColumnSpan): a thread writes
+// the lower faces of its cells, and the wall face beyond the last cell along an axis.  The solution is read from one buffer and the
 // mean-removed potential written to another, since every thread also reads its neighbours' values.
 template <class T> struct FinishArgs {
     Params p;
@@ -678,35 +720,72 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
         }
     }
     const double mean = c->phi_sum / p.n_cell;
-    const int sy = p.nx, sz = p.nx * p.ny;
-    auto pv = [&](int j) { return zero_phi ? 0.0 : a.phi[j] - mean; };
-    for (int i = err ? p.n_cell : k.x * kThreads + threadIdx.x; i < p.n_cell; i += k.nx * kThreads) {
-        const int x = i % p.nx, y = (i / p.nx) % p.ny, z = i / (p.nx * p.ny);
-        const double ph = pv(i);
-        // faces below this cell (wall faces 0), and above it at the last cell of an axis
-        const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
-        T uf[2], vf[2], wf[2];
-        uf[0] = x == 0 ? T(0) : a.m[X][iu] - (T)((ph - pv(i - 1)) * a.g.dinv_sp[X][x]);
-        vf[0] = y == 0 ? T(0) : a.m[Y][iv] - (T)((ph - pv(i - sy)) * a.g.dinv_sp[Y][y]);
-        wf[0] = z == 0 ? T(0) : a.m[Z][iw] - (T)((ph - pv(i - sz)) * a.g.dinv_sp[Z][z]);
-        uf[1] = x == p.nx - 1 ? T(0) : a.m[X][iu + 1] - (T)((pv(i + 1) - ph) * a.g.dinv_sp[X][x + 1]);
-        vf[1] = y == p.ny - 1 ? T(0) : a.m[Y][iv + p.nx] - (T)((pv(i + sy) - ph) * a.g.dinv_sp[Y][y + 1]);
-        wf[1] = z == p.nz - 1 ? T(0) : a.m[Z][iw + sz] - (T)((pv(i + sz) - ph) * a.g.dinv_sp[Z][z + 1]);
-        a.u_out[X][iu] = uf[0];
-        a.u_out[Y][iv] = vf[0];
-        a.u_out[Z][iw] = wf[0];
-        if (x == p.nx - 1) a.u_out[X][iu + 1] = uf[1];
-        if (y == p.ny - 1) a.u_out[Y][iv + p.nx] = vf[1];
-        if (z == p.nz - 1) a.u_out[Z][iw + sz] = wf[1];
-        if (a.last_stage) {
-            // CFL rate of the new velocity, as backend.cu:469-471 (divisions kept for identical rounding)
-            const T r = fmax(fabs(uf[0]), fabs(uf[1])) / tab(a.g, X, kW, x) +
-                        fmax(fabs(vf[0]), fabs(vf[1])) / tab(a.g, Y, kW, y) +
-                        fmax(fabs(wf[0]), fabs(wf[1])) / tab(a.g, Z, kW, z);
-            acc.v[0] = combine<1, true>(acc.v[0], (double)r);
+    auto pv = [&](int j) { return zero_phi ? 0.0 : __ldg(a.phi + j) - mean; };
+    const ColumnSpan cs = column_span(p, k);
+    if (!err && cs.live && cs.z0 < cs.z1) {
+        const int x = cs.x, y = cs.y, nx = p.nx, sy = p.nx, sz = p.nx * p.ny;
+        const int su = (p.nx + 1) * p.ny, sv = p.nx * (p.ny + 1);     // layer strides of the u and v faces
+        const bool xl = x > 0, xh = x + 1 < p.nx, yl = y > 0, yh = y + 1 < p.ny;
+        const double ixl = a.g.dinv_sp[X][x], ixh = a.g.dinv_sp[X][x + 1];
+        const double iyl = a.g.dinv_sp[Y][y], iyh = a.g.dinv_sp[Y][y + 1];
+        const T wx = tab(a.g, X, kW, x), wy = tab(a.g, Y, kW, y);
+        // the loads of a layer, issued one layer ahead of its arithmetic (the faces above the cell only for
+        // the CFL rate of the last stage)
+        const bool cfl = a.last_stage;
+        struct Layer { double above, w, s, e, n, base, izh; T mx, my, mz, mx1, my1, wz; };
+        auto fetch = [&](int j, int ju, int jv, int z) {
+            Layer v;
+            const bool zh = z + 1 < p.nz;
+            v.above = zh ? pv(j + sz) : 0.0;
+            v.w = xl ? pv(j - 1) : 0.0;
+            v.s = yl ? pv(j - sy) : 0.0;
+            v.mx = xl ? __ldg(a.m[X] + ju) : T(0);
+            v.my = yl ? __ldg(a.m[Y] + jv) : T(0);
+            v.mz = zh ? __ldg(a.m[Z] + j + sz) : T(0);
+            v.izh = zh ? __ldg(a.g.dinv_sp[Z] + z + 1) : 0.0;
+            v.base = hb >= 0 ? __ldg(a.base + j) : 0.0;
+            v.e = cfl && xh ? pv(j + 1) : 0.0;
+            v.n = cfl && yh ? pv(j + sy) : 0.0;
+            v.mx1 = cfl && xh ? __ldg(a.m[X] + ju + 1) : T(0);
+            v.my1 = cfl && yh ? __ldg(a.m[Y] + jv + nx) : T(0);
+            v.wz = cfl ? tab(a.g, Z, kW, z) : T(1);
+            return v;
+        };
+        int i = cs.p + cs.z0 * sz;
+        int iu = fidx<X>(p, x, y, cs.z0), iv = fidx<Y>(p, x, y, cs.z0);
+        double ph = pv(i);
+        T wlo = T(0);                 // the w-face below this cell, as the cell below computed it
+        if (cs.z0 > 0) wlo = __ldg(a.m[Z] + i) - (T)((ph - pv(i - sz)) * a.g.dinv_sp[Z][cs.z0]);
+        Layer next = fetch(i, iu, iv, cs.z0);
+        for (int z = cs.z0; z < cs.z1; z++, i += sz, iu += su, iv += sv) {
+            const Layer l = next;
+            if (z + 1 < cs.z1) next = fetch(i + sz, iu + su, iv + sv, z + 1);
+            // faces below this cell (wall faces 0), and above it at the last cell of an axis
+            const bool zh = z + 1 < p.nz;
+            T uf[2], vf[2], wf[2];
+            uf[0] = xl ? l.mx - (T)((ph - l.w) * ixl) : T(0);
+            vf[0] = yl ? l.my - (T)((ph - l.s) * iyl) : T(0);
+            wf[0] = wlo;
+            wf[1] = zh ? l.mz - (T)((l.above - ph) * l.izh) : T(0);
+            a.u_out[X][iu] = uf[0];
+            a.u_out[Y][iv] = vf[0];
+            a.u_out[Z][i] = wf[0];
+            if (!xh) a.u_out[X][iu + 1] = T(0);
+            if (!yh) a.u_out[Y][iv + nx] = T(0);
+            if (!zh) a.u_out[Z][i + sz] = T(0);
+            if (cfl) {
+                uf[1] = xh ? l.mx1 - (T)((l.e - ph) * ixh) : T(0);
+                vf[1] = yh ? l.my1 - (T)((l.n - ph) * iyh) : T(0);
+                // CFL rate of the new velocity, as backend.cu:469-471 (divisions kept for identical rounding)
+                const T r = fmax(fabs(uf[0]), fabs(uf[1])) / wx + fmax(fabs(vf[0]), fabs(vf[1])) / wy +
+                            fmax(fabs(wf[0]), fabs(wf[1])) / l.wz;
+                acc.v[0] = combine<1, true>(acc.v[0], (double)r);
+            }
+            a.phi_out[i] = ph;
+            if (hb >= 0) a.hist[hb][i] = 1.0 * ph + -1.0 * l.base;
+            wlo = wf[1];
+            ph = l.above;
         }
-        a.phi_out[i] = ph;
-        if (hb >= 0) a.hist[hb][i] = 1.0 * ph + -1.0 * a.base[i];
     }
     // gridwide: CFL max (NaN wins) and the scalar bookkeeping in the last block
     const Vec<1> blk = block_reduce<1, true>(acc);

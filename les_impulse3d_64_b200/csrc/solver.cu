@@ -550,17 +550,11 @@ private:
         check(cudaGetDevice(&dev));
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         sms_ = sms;
-        cell_blocks_ = (unsigned int)std::min<long long>(blocks_for(n_cell_), 4LL * sms);
-        // the grid-stride cell kernels: as many CTAs as fit on the device at once (latency-bound loads want every
-        // resident warp), and never more than one cell per thread
-        auto resident = [&](const void* fn) {
-            int per_sm = 4;
-            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
-            return (unsigned int)std::min<long long>(blocks_for(n_cell_), (long long)std::max(per_sm, 1) * sms);
-        };
-        start_blocks_ = resident((const void*)projection_start_kernel<T>);
+        // the column kernels: how many of their blocks an SM holds (their grids fill the device that deep)
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&start_per_sm_, (const void*)projection_start_kernel<T>,
+                                                            kThreads, 0));
         check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&residual_per_sm_, (const void*)residual_kernel, kThreads, 0));
-        finish_blocks_ = resident((const void*)finish_kernel<T>);
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&finish_per_sm_, (const void*)finish_kernel<T>, kThreads, 0));
         if (tc_fdm_) {
             inv_lambda_f_ = arena_.alloc<float>(n_cell_);
             const int n[3] = {nx_, ny_, nz_};
@@ -709,9 +703,6 @@ private:
     }
 
     // ------------------------------------------------------------------------------ kernel launches
-    // grid of a recorded cell kernel: in a batch the launch already spans many cavities, so each cavity keeps
-    // the smaller grid (fewer partials per reduction)
-    unsigned int cell_grid(unsigned int alone) const { return g_launch_batch > 1 ? cell_blocks_ : alone; }
     // grid of a column kernel (ColumnSpan): plane blocks along x and z-chunks along y, as many chunks as it takes
     // for the launch (all cavities of a batch together) to fill the device `per_sm` blocks deep
     dim3 column_grid(int per_sm) const {
@@ -777,11 +768,14 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        if (!record_launch(kLkStart, 0, dim3(cell_grid(start_blocks_)), 0, a))
-            check(launch_pdl(projection_start_kernel<T>, dim3(start_blocks_), dim3(kThreads), 0, st, a));
+        const dim3 grid = column_grid(start_per_sm_);
+        if (!record_launch(kLkStart, 0, grid, 0, a))
+            check(launch_pdl(projection_start_kernel<T>, grid, dim3(kThreads), 0, st, a));
+        if (step_mode) launch_residual(st, praw_, h, use_h, 1);    // the residual of the guess
     }
-    void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, int use_h) {
+    void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, int use_h, int start = 0) {
         ResidualArgs a;
+        a.start = start;
         a.p = p_;
         for (int k = 0; k < 3; k++) { a.dw[k] = geo_.dw[k]; a.dinv_sp[k] = geo_.dinv_sp[k]; }
         a.phi = phi;
@@ -819,8 +813,8 @@ private:
         a.stage = stage;
         a.c = ctrl_;
         a.partial = partial_;
-        if (!record_launch(kLkFinish, 0, dim3(cell_grid(finish_blocks_)), 0, a))
-            check(launch_pdl(finish_kernel<T>, dim3(finish_blocks_), dim3(kThreads), 0, st, a));
+        const dim3 grid = column_grid(finish_per_sm_);
+        if (!record_launch(kLkFinish, 0, grid, 0, a)) check(launch_pdl(finish_kernel<T>, grid, dim3(kThreads), 0, st, a));
     }
 
     // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
@@ -967,9 +961,7 @@ private:
     TcFdmOperands tcop_ = {};
     double* partial_;
     long long partial_blocks_;
-    unsigned int cell_blocks_ = 1;     // grid of other grid-stride cell kernels: at most 4 CTAs per SM
-    unsigned int start_blocks_ = 1, finish_blocks_ = 1;
-    int residual_per_sm_ = 1;
+    int residual_per_sm_ = 1, start_per_sm_ = 1, finish_per_sm_ = 1;
     Control* ctrl_;
     double *slots_, *stats_, *line_, *dstage_[2];
     unsigned int* out_counters_;
