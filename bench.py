@@ -171,6 +171,18 @@ def momentum_bytes(settings, field_bytes):
     return 4 * faces * field_bytes
 
 
+def cell_kernel_bytes(settings, field_bytes):
+    """Algorithmic HBM bytes of one launch of each cell kernel of a step's projection, each array element once:
+    projection start (read m and, in every stage, two potentials and two history increments; write rhs, base,
+    guess and in stage 0 phi0 for the other two: 3f + 56 per cell), residual (read phi and rhs, write r: 24 per
+    cell) and finish (read phi, m and base, write u, phi and the history increment: 6f + 32 per cell)."""
+    nx, ny, nz = settings['nx'], settings['ny'], settings['nz']
+    cells = nx * ny * nz
+    faces = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+    return {'projection_start': faces * field_bytes + 56 * cells, 'guess_residual': 24 * cells,
+            'finish': 2 * faces * field_bytes + 32 * cells}
+
+
 def cpu_oracle_rate(workload, steps_budget_s=12.0, max_steps=40):
     """The FP64 OpenMP oracle on this host: cell-updates/s over a bounded number of steps."""
     from les_impulse3d_64_b200 import workloads
@@ -238,6 +250,7 @@ def run_ours(args, ranks):
     ranks.barrier()
     with ClockSampler(ranks.local) as clocks:
         ms, kms = cav.time_steps(args.warmup, args.steps, flush_l2=True)
+    ktimes = cav.kernel_times()
     passes = cav.pressure_passes() - passes0
     device_bytes = cav.device_bytes()
     launches = args.steps * cav.kernels_per_step(0) + 7 * passes_in_timed(passes, args, cav)
@@ -282,6 +295,13 @@ def run_ours(args, ranks):
     peak, peak_kind = measured_peaks()
     kernel_s = float(kms.sum()) / 1e3 / (3 * args.steps)
     achieved = momentum_bytes(s, field_bytes) / kernel_s / 1e9
+    # the other stencil kernels of the step, timed by events in the same graph (their launches in all stages)
+    cell_kernels = {}
+    for name, nbytes in cell_kernel_bytes(s, field_bytes).items():
+        launch_s = ranks.max(ktimes[name]) / 1e3 / 3
+        gbs = nbytes / launch_s / 1e9 if launch_s > 0 else None
+        cell_kernels[name] = {'ms_per_launch': launch_s * 1e3, 'bytes_per_launch': nbytes, 'achieved_gbs': gbs,
+                              'frac': gbs / peak if gbs else None}
     line = {
         'metric': 'cell-updates/s per RK3 step', 'value': value, 'unit': 'cell-updates/s', 'n_gpus': ranks.world,
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
@@ -296,10 +316,11 @@ def run_ours(args, ranks):
         'e2e_queued_outputs': {'value': ranks.world * cells * args.steps / queued_s, 'unit': 'cell-updates/s',
                                'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
         'gpu_launches': launches,
-        'pressure_passes_per_stage': passes / (3 * (args.steps + args.warmup)) if args.steps else None,
+        'pressure_passes_per_stage': passes / (3 * (2 * args.steps + args.warmup)) if args.steps else None,
         'roofline': {'kernel': sweep_kernel_name(), 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                      'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': profile_traffic(args.workload), 'ms_per_launch': kernel_s * 1e3},
+        'stencil_kernels': cell_kernels,
         'clocks': clocks.summary(),
     }
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
@@ -316,8 +337,8 @@ def replica_rate(world, cells, steps, max_ms):
 
 
 def passes_in_timed(passes, args, cav):
-    # passes counted over warm-up + timed steps; scale to the timed steps
-    total = args.steps + args.warmup
+    # passes counted over warm-up, timed steps and the kernel-timing steps after them; scale to the timed steps
+    total = 2 * args.steps + args.warmup
     return int(round(passes * args.steps / total)) if total else 0
 
 

@@ -96,9 +96,14 @@ long long cavity_estimate_bytes(const CavityConfig* config, int precision);
 
 /* Timing support for benchmarks: run `warmup` untimed steps, then `steps` steps, each bracketed by CUDA
  * events on the solver's stream, with the L2 cache flushed (a 256 MiB device write) before each timed
- * step when flush_l2 != 0.  ms_per_step[steps] receives each step's device time; kernel_ms[steps] (may be
- * NULL) the device time of the momentum-sweep launches inside that step. */
+ * step when flush_l2 != 0.  ms_per_step[steps] receives each step's device time.  When kernel_ms is not NULL,
+ * `steps` more steps follow through a step graph that also records events around the kernels; kernel_ms[steps]
+ * receives the device time of each one's momentum-sweep launches (see also cavity_kernel_times). */
 int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms_per_step, float* kernel_ms);
+/* After cavity_time_steps: ms[4] receives the mean device time per timed step (milliseconds, all three stages)
+ * of the momentum sweeps, the projection starts, the residuals of their warm-start guesses, and the finishes.
+ * No counterpart in the reference. */
+int cavity_kernel_times(CavitySolver* s, double* ms);
 /* The handle of the process-wide solver behind the solver_* functions (NULL if none). */
 CavitySolver* cavity_default(void);
 /* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */

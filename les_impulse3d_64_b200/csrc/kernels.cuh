@@ -195,6 +195,8 @@ __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockI
 // Cells visited as columns: a block takes kThreads consecutive cells of an x-y plane (x fastest) and walks them
 // up a chunk of z-layers; grid y runs over the chunks.  A thread's plane position, and so its x and y table
 // values, stay fixed, and its column's values below and at the current layer carry over in registers.
+// blocks of a column kernel an SM is to hold: its loads run one layer ahead, so occupancy is its memory parallelism
+constexpr int kColumnBlocks = 4;
 struct ColumnSpan {
     int p, x, y, z0, z1;
     bool live;
@@ -526,11 +528,11 @@ __device__ void projection_start_body(const StartArgs<T>& a, const Blk& k) {
     }
 }
 template <class T>
-__global__ void __launch_bounds__(kThreads) projection_start_kernel(StartArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_kernel(StartArgs<T> a) {
     projection_start_body(a, real_blk());
 }
 template <class T>
-__global__ void __launch_bounds__(kThreads) projection_start_batched(const StartArgs<T>* args) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_batched(const StartArgs<T>* args) {
     __shared__ StartArgs<T> a;
     int cav;
     const Blk k = batch_blk(1, cav);
@@ -575,19 +577,15 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
         const bool xl = x > 0, xh = x + 1 < p.nx, yl = y > 0, yh = y + 1 < p.ny;
         const double ixl = a.dinv_sp[X][x], ixh = a.dinv_sp[X][x + 1], iyl = a.dinv_sp[Y][y], iyh = a.dinv_sp[Y][y + 1];
         const double* f = a.phi;
-        // the loads of a layer, issued one layer ahead of its arithmetic
-        struct Layer { double above, e, w, n, s, rhs, dz, izl, izh; };
+        // the loads of a layer that go to DRAM or to other blocks' rows, issued one layer ahead of its arithmetic;
+        // the same row's neighbours and the z tables are L1 hits by then
+        struct Layer { double above, n, s, rhs; };
         auto fetch = [&](int j, int z) {
             Layer v;
             v.above = z + 1 < p.nz ? __ldg(f + j + sz) : 0.0;
-            v.e = xh ? __ldg(f + j + 1) : 0.0;
-            v.w = xl ? __ldg(f + j - 1) : 0.0;
             v.n = yh ? __ldg(f + j + sy) : 0.0;
             v.s = yl ? __ldg(f + j - sy) : 0.0;
             v.rhs = __ldg(a.rhs + j);
-            v.dz = __ldg(a.dw[Z] + z);
-            v.izl = __ldg(a.dinv_sp[Z] + z);
-            v.izh = __ldg(a.dinv_sp[Z] + z + 1);
             return v;
         };
         int i = cs.p + cs.z0 * sz;
@@ -597,14 +595,14 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
         for (int z = cs.z0; z < cs.z1; z++, i += sz) {
             const Layer l = next;
             if (z + 1 < cs.z1) next = fetch(i + sz, z + 1);
-            const double dz = l.dz;
+            const double dz = __ldg(a.dw[Z] + z);
             double s = 0.0;
-            if (xh) s += (dy * dz) * (l.e - cc) * ixh;
-            if (xl) s -= (dy * dz) * (cc - l.w) * ixl;
+            if (xh) s += (dy * dz) * (__ldg(f + i + 1) - cc) * ixh;
+            if (xl) s -= (dy * dz) * (cc - __ldg(f + i - 1)) * ixl;
             if (yh) s += (dx * dz) * (l.n - cc) * iyh;
             if (yl) s -= (dx * dz) * (cc - l.s) * iyl;
-            if (z + 1 < p.nz) s += (dx * dy) * (l.above - cc) * l.izh;
-            if (z > 0) s -= (dx * dy) * (cc - below) * l.izl;
+            if (z + 1 < p.nz) s += (dx * dy) * (l.above - cc) * __ldg(a.dinv_sp[Z] + z + 1);
+            if (z > 0) s -= (dx * dy) * (cc - below) * __ldg(a.dinv_sp[Z] + z);
             const double r = l.rhs - s;
             a.res[i] = r;
             acc.v[0] += r * r;
@@ -645,8 +643,8 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
         }
     }
 }
-__global__ void __launch_bounds__(kThreads) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
-__global__ void __launch_bounds__(kThreads) residual_batched(const ResidualArgs* args) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) residual_batched(const ResidualArgs* args) {
     __shared__ ResidualArgs a;
     int cav;
     const Blk k = batch_blk(1, cav);
@@ -729,26 +727,22 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
         const double ixl = a.g.dinv_sp[X][x], ixh = a.g.dinv_sp[X][x + 1];
         const double iyl = a.g.dinv_sp[Y][y], iyh = a.g.dinv_sp[Y][y + 1];
         const T wx = tab(a.g, X, kW, x), wy = tab(a.g, Y, kW, y);
-        // the loads of a layer, issued one layer ahead of its arithmetic (the faces above the cell only for
-        // the CFL rate of the last stage)
+        // the loads of a layer that go to DRAM or to other blocks' rows, issued one layer ahead of its arithmetic;
+        // the same row's neighbours and the z tables are L1 hits by then (the faces above the cell are needed only
+        // for the CFL rate of the last stage)
         const bool cfl = a.last_stage;
-        struct Layer { double above, w, s, e, n, base, izh; T mx, my, mz, mx1, my1, wz; };
+        struct Layer { double above, s, n, base; T mx, my, mz, my1; };
         auto fetch = [&](int j, int ju, int jv, int z) {
             Layer v;
             const bool zh = z + 1 < p.nz;
             v.above = zh ? pv(j + sz) : 0.0;
-            v.w = xl ? pv(j - 1) : 0.0;
             v.s = yl ? pv(j - sy) : 0.0;
-            v.mx = xl ? __ldg(a.m[X] + ju) : T(0);
-            v.my = yl ? __ldg(a.m[Y] + jv) : T(0);
-            v.mz = zh ? __ldg(a.m[Z] + j + sz) : T(0);
-            v.izh = zh ? __ldg(a.g.dinv_sp[Z] + z + 1) : 0.0;
-            v.base = hb >= 0 ? __ldg(a.base + j) : 0.0;
-            v.e = cfl && xh ? pv(j + 1) : 0.0;
             v.n = cfl && yh ? pv(j + sy) : 0.0;
-            v.mx1 = cfl && xh ? __ldg(a.m[X] + ju + 1) : T(0);
+            v.base = hb >= 0 ? __ldg(a.base + j) : 0.0;
+            v.mx = __ldg(a.m[X] + ju);
+            v.my = __ldg(a.m[Y] + jv);
+            v.mz = zh ? __ldg(a.m[Z] + j + sz) : T(0);
             v.my1 = cfl && yh ? __ldg(a.m[Y] + jv + nx) : T(0);
-            v.wz = cfl ? tab(a.g, Z, kW, z) : T(1);
             return v;
         };
         int i = cs.p + cs.z0 * sz;
@@ -763,10 +757,10 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
             // faces below this cell (wall faces 0), and above it at the last cell of an axis
             const bool zh = z + 1 < p.nz;
             T uf[2], vf[2], wf[2];
-            uf[0] = xl ? l.mx - (T)((ph - l.w) * ixl) : T(0);
+            uf[0] = xl ? l.mx - (T)((ph - pv(i - 1)) * ixl) : T(0);
             vf[0] = yl ? l.my - (T)((ph - l.s) * iyl) : T(0);
             wf[0] = wlo;
-            wf[1] = zh ? l.mz - (T)((l.above - ph) * l.izh) : T(0);
+            wf[1] = zh ? l.mz - (T)((l.above - ph) * __ldg(a.g.dinv_sp[Z] + z + 1)) : T(0);
             a.u_out[X][iu] = uf[0];
             a.u_out[Y][iv] = vf[0];
             a.u_out[Z][i] = wf[0];
@@ -774,11 +768,11 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
             if (!yh) a.u_out[Y][iv + nx] = T(0);
             if (!zh) a.u_out[Z][i + sz] = T(0);
             if (cfl) {
-                uf[1] = xh ? l.mx1 - (T)((l.e - ph) * ixh) : T(0);
+                uf[1] = xh ? __ldg(a.m[X] + iu + 1) - (T)((pv(i + 1) - ph) * ixh) : T(0);
                 vf[1] = yh ? l.my1 - (T)((l.n - ph) * iyh) : T(0);
                 // CFL rate of the new velocity, as backend.cu:469-471 (divisions kept for identical rounding)
                 const T r = fmax(fabs(uf[0]), fabs(uf[1])) / wx + fmax(fabs(vf[0]), fabs(vf[1])) / wy +
-                            fmax(fabs(wf[0]), fabs(wf[1])) / l.wz;
+                            fmax(fabs(wf[0]), fabs(wf[1])) / tab(a.g, Z, kW, z);
                 acc.v[0] = combine<1, true>(acc.v[0], (double)r);
             }
             a.phi_out[i] = ph;
@@ -822,9 +816,9 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
     }
 }
 template <class T>
-__global__ void __launch_bounds__(kThreads) finish_kernel(FinishArgs<T> a) { finish_body(a, real_blk()); }
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_kernel(FinishArgs<T> a) { finish_body(a, real_blk()); }
 template <class T>
-__global__ void __launch_bounds__(kThreads) finish_batched(const FinishArgs<T>* args) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_batched(const FinishArgs<T>* args) {
     __shared__ FinishArgs<T> a;
     int cav;
     const Blk k = batch_blk(1, cav);

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -110,6 +111,7 @@ public:
     virtual void q_volume(int colour_w, float* q, float* colour) = 0;
     virtual long long device_bytes() const = 0;
     virtual void time_steps(int warmup, int steps, int flush, float* ms, float* kms) = 0;
+    virtual void kernel_times(double* ms) const = 0;
     virtual int kernels_per_step(int passes) const = 0;
     virtual long long pressure_passes() const = 0;
     void step(CavityReport* r) {
@@ -478,34 +480,52 @@ public:
     int kernels_per_step(int passes) const override { return 1 + 3 * 3 + 3 * passes * 7; }
     long long pressure_passes() const override { return hc_.pass_count; }
 
+    // `steps` steps through the plain step graph, each timed by events around its launch; then, when `kms` is
+    // given, `steps` more through the graph with events around the kernels (they cost launch latency, so the step
+    // times come from the plain graph), for the per-kernel times
     void time_steps(int warmup, int steps, int flush, float* ms, float* kms) override {
         if (flush && !flush_) check(cudaMalloc(&flush_, kFlushBytes));
-        ensure_graphs(true);
+        ensure_graphs(false);
+        if (kms) ensure_graphs(true);
         for (int i = 0; i < warmup; i++) step(nullptr);
+        for (double& t : timed_ms_) t = 0;
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0));
         check(cudaEventCreate(&e1));
-        for (int i = 0; i < steps; i++) {
-            if (flush) check(cudaMemsetAsync(flush_, i & 0xff, kFlushBytes, stream_));
-            check(cudaEventRecord(e0, stream_));
-            if (eager_) enqueue_step(par_, true, true);
-            else check(cudaGraphLaunch(texec_[par_], stream_));
-            pending_.push_back(par_);
-            par_ ^= 1;
-            check(cudaEventRecord(e1, stream_));
-            sync(nullptr);
-            check(cudaEventElapsedTime(&ms[i], e0, e1));
-            if (kms) {
-                float tot = 0, t;
-                for (int s = 0; s < 3; s++) {
-                    check(cudaEventElapsedTime(&t, kev_[2 * s], kev_[2 * s + 1]));
-                    tot += t;
+        for (int pass = 0; pass < (kms ? 2 : 1); pass++) {
+            const bool timing = pass == 1;
+            for (int i = 0; i < steps; i++) {
+                if (flush) check(cudaMemsetAsync(flush_, i & 0xff, kFlushBytes, stream_));
+                check(cudaEventRecord(e0, stream_));
+                if (eager_) enqueue_step(par_, timing, true);
+                else check(cudaGraphLaunch(timing ? texec_[par_] : exec_[par_], stream_));
+                pending_.push_back(par_);
+                par_ ^= 1;
+                check(cudaEventRecord(e1, stream_));
+                sync(nullptr);
+                if (!timing) {
+                    check(cudaEventElapsedTime(&ms[i], e0, e1));
+                    continue;
                 }
-                kms[i] = tot;
+                for (int kind = 0; kind < kNumTimed; kind++) {
+                    float tot = 0, t;
+                    for (int s = 0; s < 3; s++) {
+                        check(cudaEventElapsedTime(&t, kev(kind, s)[0], kev(kind, s)[1]));
+                        tot += t;
+                    }
+                    timed_ms_[kind] += tot / steps;
+                    if (kind == kTkSweep) kms[i] = tot;
+                }
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+    }
+
+    // per-step device time of the sweeps, the projection starts, the residuals of their guesses and the finishes
+    // (all three stages) in the last time_steps call
+    void kernel_times(double* ms) const override {
+        for (int k = 0; k < kNumTimed; k++) ms[k] = timed_ms_[k];
     }
 
 private:
@@ -709,7 +729,7 @@ private:
         const long long bpp = blocks_for((long long)nx_ * ny_);
         const long long want = (long long)sms_ * std::max(per_sm, 1);
         const long long cav = std::max(g_launch_batch, 1);
-        long long chunks = std::min<long long>(nz_, std::max(1LL, (want + bpp * cav - 1) / (bpp * cav)));
+        long long chunks = std::min<long long>(nz_, std::max(1LL, want / (bpp * cav)));
         const long long zc = (nz_ + chunks - 1) / chunks;
         chunks = (nz_ + zc - 1) / zc;
         return dim3((unsigned int)bpp, (unsigned int)chunks);
@@ -748,9 +768,10 @@ private:
         }
     }
     // rhs, starting potential and its residual, start-of-solve decisions (backend.cu:816-831)
-    // use_h: 0 no graph loop, 1 this solver's own loop, 2 a loop shared by a batch (see set_loop)
+    // use_h: 0 no graph loop, 1 this solver's own loop, 2 a loop shared by a batch (see set_loop); `between` runs
+    // between the start kernel and the residual of the guess (timing events)
     void launch_start(cudaStream_t st, T* const m[3], bool step_mode, int stage, int S, int cur,
-                      cudaGraphConditionalHandle h, int use_h) {
+                      cudaGraphConditionalHandle h, int use_h, const std::function<void()>& between = {}) {
         StartArgs<T> a;
         a.p = p_;
         a.g = geo_;
@@ -771,6 +792,7 @@ private:
         const dim3 grid = column_grid(start_per_sm_);
         if (!record_launch(kLkStart, 0, grid, 0, a))
             check(launch_pdl(projection_start_kernel<T>, grid, dim3(kThreads), 0, st, a));
+        if (between) between();
         if (step_mode) launch_residual(st, praw_, h, use_h, 1);    // the residual of the guess
     }
     void launch_residual(cudaStream_t st, const double* phi, cudaGraphConditionalHandle h, int use_h, int start = 0) {
@@ -858,22 +880,36 @@ private:
             const int in = stage == 0 ? S : stage == 1 ? Xs : Ys;
             const int out = stage == 1 ? Ys : Xs;
             const int cur = stage == 1 ? Xs : Ys;          // potential of the previous stage (stages 1, 2)
-            if (timing) mark(kev_[2 * stage]);
+            if (timing) mark(kev(kTkSweep, stage)[0]);
             launch_momentum(stream_, stage, S, in, out);
-            if (timing) mark(kev_[2 * stage + 1]);
+            if (timing) mark(kev(kTkSweep, stage)[1]);
             double* phi = praw_;          // the solve works here; finish writes PHI_[out]
+            // with timing: events around the projection start and around the residual of its guess
+            std::function<void()> between;
+            if (timing) {
+                mark(kev(kTkStart, stage)[0]);
+                between = [&, stage] {
+                    mark(kev(kTkStart, stage)[1]);
+                    mark(kev(kTkGuessResidual, stage)[0]);
+                };
+            }
             if (eager) {
-                launch_start(stream_, M_[out], true, stage, S, cur, 0, 0);
+                launch_start(stream_, M_[out], true, stage, S, cur, 0, 0, between);
+                if (timing) mark(kev(kTkGuessResidual, stage)[1]);
                 pull_control();
                 while (hc_.cond && !hc_.error) {
                     launch_pass(stream_, phi, 0, 0);
                     pull_control();
                 }
             } else {
-                captured_loop([&](cudaGraphConditionalHandle h) { launch_start(stream_, M_[out], true, stage, S, cur, h, 1); },
-                              phi);
+                captured_loop([&](cudaGraphConditionalHandle h) {
+                    launch_start(stream_, M_[out], true, stage, S, cur, h, 1, between);
+                    if (timing) mark(kev(kTkGuessResidual, stage)[1]);
+                }, phi);
             }
+            if (timing) mark(kev(kTkFinish, stage)[0]);
             launch_finish(stream_, M_[out], U_[out], PHI_[out], true, stage, stage == 2);
+            if (timing) mark(kev(kTkFinish, stage)[1]);
         }
     }
 
@@ -970,7 +1006,11 @@ private:
     const double* centre_[3];
     cudaGraph_t graph_[2] = {nullptr, nullptr}, tgraph_[2] = {nullptr, nullptr};
     cudaGraphExec_t exec_[2] = {nullptr, nullptr}, texec_[2] = {nullptr, nullptr};
-    cudaEvent_t kev_[6] = {};
+    // events of the timing graph: [kernel][stage][begin, end]; per-step means of the last time_steps call
+    enum TimedKernel : int { kTkSweep = 0, kTkStart, kTkGuessResidual, kTkFinish, kNumTimed };
+    cudaEvent_t kev_[2 * 3 * kNumTimed] = {};
+    cudaEvent_t* kev(int kind, int stage) { return kev_ + 2 * (3 * kind + stage); }
+    double timed_ms_[kNumTimed] = {};
     void* flush_ = nullptr;
     float* ring_host_ = nullptr;       // queued per-step probe values (pinned, mapped)
     float* ring_dev_ = nullptr;
@@ -1447,6 +1487,9 @@ long long cavity_estimate_bytes(const CavityConfig* config, int precision) {
 }
 int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms, float* kms) {
     return safely([&] { H(s).time_steps(warmup, steps, flush_l2, ms, kms); });
+}
+int cavity_kernel_times(CavitySolver* s, double* ms) {
+    return safely([&] { H(s).kernel_times(ms); });
 }
 CavitySolver* cavity_default(void) { return g_default; }
 int cavity_step_outputs_async(CavitySolver* s, int count, int statistics) {
