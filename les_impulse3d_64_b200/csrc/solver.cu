@@ -477,7 +477,8 @@ public:
     }
     long long device_bytes() const override { return arena_.bytes(); }
 
-    int kernels_per_step(int passes) const override { return 1 + 3 * 3 + 3 * passes * 7; }
+    // step begin; per stage the sweep, the projection start, the residual of its guess and the finish; 7 per pass
+    int kernels_per_step(int passes) const override { return 1 + 3 * 4 + 3 * passes * 7; }
     long long pressure_passes() const override { return hc_.pass_count; }
 
     // `steps` steps through the plain step graph, each timed by events around its launch; then, when `kms` is
