@@ -19,7 +19,7 @@
 // thread issues the tcgen05.mma.cta_group::1.kind::tf32 instructions (M = 128, N = BN, K = 8) and commits each
 // panel to that stage's mbarrier.  Every mbarrier wait is bounded: on time-out the kernel records
 // kDeviceWait in the control block, frees its TMEM and returns.  Only this kernel allocates TMEM, and the
-// shared memory of a CTA (>= 80 KB) keeps at most 2 CTAs of <= 128 columns on an SM, below its 512 columns.
+// shared memory of a CTA (>= 80 KB) keeps at most 2 CTAs of <= 64 columns on an SM, below its 512 columns.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -447,12 +447,11 @@ __global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTrans
 }
 
 // ---------------------------------------------------------------- host side
-// tile width: the widest of 128 / 64 / 32 columns that still gives one CTA per SM, else 32
+// tile width: 64 columns when that still gives one CTA per SM, else 32.  (128-column tiles would need 128 KB of
+// shared memory, one CTA per SM, and each CTA's K loop is latency-bound: two CTAs per SM of 64 columns are faster.)
 inline int tc_pick_bn(int M, int N, int batch, int sms) {
     const long long mt = (M + kTcRows - 1) / kTcRows;
-    for (int bn : {128, 64})
-        if ((long long)((N + bn - 1) / bn) * mt * batch >= sms) return bn;
-    return 32;
+    return (long long)((N + 63) / 64) * mt * batch >= sms ? 64 : 32;
 }
 // once per device, before any capture: the dynamic shared memory of every instance
 template <int BN> inline cudaError_t tc_prepare_bn() {
@@ -478,8 +477,7 @@ template <int BN> inline cudaError_t tc_prepare_batched_bn() {
     return e;
 }
 inline cudaError_t tc_transform_prepare_batched() {
-    cudaError_t e = tc_prepare_batched_bn<128>();
-    if (e == cudaSuccess) e = tc_prepare_batched_bn<64>();
+    cudaError_t e = tc_prepare_batched_bn<64>();
     if (e == cudaSuccess) e = tc_prepare_batched_bn<32>();
     return e;
 }
@@ -493,13 +491,11 @@ inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, unsigned int per, c
 // a recorded launch (variant: see tc_variant) over a batch of cavities
 inline void launch_tc_batched(int variant, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
     const int bn = variant & 0xff, fa = (variant >> 8) & 1, f64 = (variant >> 9) & 1;
-    if (bn == 128) launch_tc_batched_bn<128>(fa, f64, grid, per, d, st);
-    else if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, per, d, st);
+    if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, per, d, st);
     else launch_tc_batched_bn<32>(fa, f64, grid, per, d, st);
 }
 inline cudaError_t tc_transform_prepare() {
-    cudaError_t e = tc_prepare_bn<128>();
-    if (e == cudaSuccess) e = tc_prepare_bn<64>();
+    cudaError_t e = tc_prepare_bn<64>();
     if (e == cudaSuccess) e = tc_prepare_bn<32>();
     return e;
 }
@@ -514,11 +510,9 @@ inline int tc_variant(int bn, const TcTransformArgs& g) { return bn | (g.field_i
 inline void launch_tc_transform(cudaStream_t st, const TcTransformArgs& g, int batch, int sms) {
     const int bn = tc_pick_bn(g.M, g.N, batch * g_launch_batch, sms);
     const dim3 grid((g.N + bn - 1) / bn, (g.M + kTcRows - 1) / kTcRows, batch);
-    if (record_launch(kLkTc, tc_variant(bn, g), grid, (size_t)(bn == 128 ? TcSmem<128>::kBytes : bn == 64 ? TcSmem<64>::kBytes
-                                                                                                       : TcSmem<32>::kBytes), g))
+    if (record_launch(kLkTc, tc_variant(bn, g), grid, (size_t)(bn == 64 ? TcSmem<64>::kBytes : TcSmem<32>::kBytes), g))
         return;
-    if (bn == 128) launch_tc_bn<128>(st, g, grid);
-    else if (bn == 64) launch_tc_bn<64>(st, g, grid);
+    if (bn == 64) launch_tc_bn<64>(st, g, grid);
     else launch_tc_bn<32>(st, g, grid);
 }
 
