@@ -213,6 +213,10 @@ __device__ __forceinline__ ColumnSpan column_span(const Params& p, const Blk& k)
     s.z1 = min(p.nz, s.z0 + zc);
     return s;
 }
+// Layers of a column walk that are brought into L2 ahead of the one whose loads go out into registers: the L2
+// prefetch holds no register, so it deepens the walk's memory parallelism for free.
+constexpr int kColumnL2Ahead = 3;
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 // Programmatic dependent launch: the step kernels are launched so that the next kernel may start while this one
 // finishes.  Every step kernel lets its dependents launch at entry and waits for its predecessor to complete
 // (with all its memory visible) before it reads anything a predecessor wrote.  Both are no-ops for a kernel
@@ -595,6 +599,11 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
         for (int z = cs.z0; z < cs.z1; z++, i += sz) {
             const Layer l = next;
             if (z + 1 < cs.z1) next = fetch(i + sz, z + 1);
+            if (z + 1 + kColumnL2Ahead < cs.z1) {
+                const int j = i + (1 + kColumnL2Ahead) * sz;
+                prefetch_l2(a.rhs + j);
+                if (z + 2 + kColumnL2Ahead < p.nz) prefetch_l2(f + j + sz);
+            }
             const double dz = __ldg(a.dw[Z] + z);
             double s = 0.0;
             if (xh) s += (dy * dz) * (__ldg(f + i + 1) - cc) * ixh;
@@ -754,6 +763,15 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
         for (int z = cs.z0; z < cs.z1; z++, i += sz, iu += su, iv += sv) {
             const Layer l = next;
             if (z + 1 < cs.z1) next = fetch(i + sz, iu + su, iv + sv, z + 1);
+            if (z + 1 + kColumnL2Ahead < cs.z1) {
+                constexpr int d = 1 + kColumnL2Ahead;
+                const int j = i + d * sz;
+                prefetch_l2(a.m[X] + iu + d * su);
+                prefetch_l2(a.m[Y] + iv + d * sv);
+                prefetch_l2(a.m[Z] + j + sz);
+                if (!zero_phi && z + 2 + kColumnL2Ahead < p.nz) prefetch_l2(a.phi + j + sz);
+                if (hb >= 0) prefetch_l2(a.base + j);
+            }
             // faces below this cell (wall faces 0), and above it at the last cell of an axis
             const bool zh = z + 1 < p.nz;
             T uf[2], vf[2], wf[2];
