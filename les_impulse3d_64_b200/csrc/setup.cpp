@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 
 #include "layout.h"
@@ -150,10 +152,11 @@ static void tridiagonal_ql(int n, std::vector<double>& d, std::vector<double>& e
     }
 }
 
-AxisEigen axis_eigen(const AxisGrid& g) {
+void axis_tridiagonal(const AxisGrid& g, std::vector<double>& d, std::vector<double>& e) {
     const int n = g.n;
     // K: face i+1 (between cells i and i+1) couples them with 1/spacing; symmetric form W^-1/2 K W^-1/2
-    std::vector<double> d(n, 0.0), e(n, 0.0), Z;
+    d.assign(n, 0.0);
+    e.assign(n, 0.0);
     for (int i = 0; i + 1 < n; i++) {
         const double k = 1.0 / g.spacing[i + 1];
         d[i] -= k;
@@ -161,9 +164,12 @@ AxisEigen axis_eigen(const AxisGrid& g) {
         e[i] = k / std::sqrt(g.width[i] * g.width[i + 1]);
     }
     for (int i = 0; i < n; i++) d[i] /= g.width[i];
-    tridiagonal_ql(n, d, e, Z);
+}
+
+AxisEigen axis_eigen_finish(const AxisGrid& g, std::vector<double> lambda, const std::vector<double>& Z) {
+    const int n = g.n;
     AxisEigen r;
-    r.lambda = d;
+    r.lambda = std::move(lambda);
     r.zero_mode = (int)(std::max_element(r.lambda.begin(), r.lambda.end()) - r.lambda.begin());
     r.lambda[r.zero_mode] = 0.0;
     r.S.resize((size_t)n * n);
@@ -172,6 +178,20 @@ AxisEigen axis_eigen(const AxisGrid& g) {
         for (int j = 0; j < n; j++) r.S[(size_t)i * n + j] = Z[(size_t)i * n + j] * inv;
     }
     return r;
+}
+
+bool eigen_on_gpu(int n) {
+    const char* m = std::getenv("CAVITY_EIGEN");
+    if (m && std::strcmp(m, "gpu") == 0) return true;
+    if (m && std::strcmp(m, "host") == 0) return false;
+    return n >= 384;
+}
+
+AxisEigen axis_eigen(const AxisGrid& g) {
+    std::vector<double> d, e, Z;
+    axis_tridiagonal(g, d, e);
+    tridiagonal_ql(g.n, d, e, Z);
+    return axis_eigen_finish(g, std::move(d), Z);
 }
 
 // ------------------------------------------------------------------------------------------ misc

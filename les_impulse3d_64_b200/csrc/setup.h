@@ -20,13 +20,20 @@ AxisGrid make_axis_grid(const CavityConfig& c, int n, double length);
 
 // Generalised eigenbasis of the 1-D Neumann pressure operator of an axis: K S = W S diag(lambda) with
 // S^T W S = I.  S is row-major n x n (eigenvector j in column j); the largest eigenvalue (the constant
-// mode, ~0) is set to exactly 0 (backend.cu:750-767).  Computed by implicit-shift QL on the symmetric
-// tridiagonal form W^-1/2 K W^-1/2.
+// mode, ~0) is set to exactly 0 (backend.cu:750-767).  Both solvers work on the symmetric tridiagonal form
+// W^-1/2 K W^-1/2 (diagonal d, coupling e[i] of i and i+1): axis_eigen by implicit-shift QL on the host,
+// axis_eigen_gpu by bisection and inverse iteration on the GPU (eigen_gpu.cu).
 struct AxisEigen {
     std::vector<double> S, lambda;
     int zero_mode = 0;
 };
+void axis_tridiagonal(const AxisGrid& g, std::vector<double>& d, std::vector<double>& e);
+// eigenvalues and orthonormal eigenvectors Z (columns, row-major) of the tridiagonal form -> AxisEigen
+AxisEigen axis_eigen_finish(const AxisGrid& g, std::vector<double> lambda, const std::vector<double>& Z);
 AxisEigen axis_eigen(const AxisGrid& g);
+AxisEigen axis_eigen_gpu(const AxisGrid& g);
+// the eigensolver of an axis of n cells: CAVITY_EIGEN=host or =gpu forces one, else the GPU from 384 cells
+bool eigen_on_gpu(int n);
 
 // Largest viscous rate over cells, nu * sum over axes 4/(width * smaller spacing), in float as
 // backend.cu:1030-1034.

@@ -625,7 +625,7 @@ private:
         // pressure eigenbases (FP64) and 1/(lambda_x + lambda_y + lambda_z), 0 at the constant mode
         AxisEigen e[3];
         for (int a = 0; a < 3; a++) {
-            e[a] = axis_eigen(ax_[a]);
+            e[a] = eigen_on_gpu(ax_[a].n) ? axis_eigen_gpu(ax_[a]) : axis_eigen(ax_[a]);
             const int n = ax_[a].n;
             std::vector<double> st((size_t)n * n);
             for (int i = 0; i < n; i++)
@@ -1527,6 +1527,18 @@ int cavity_fdm_pass_tf32(int nx, int ny, int nz, const double* const s[3], const
 int cavity_fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                             const double* inv_lambda, const double* r, double* phi, void* stream) {
     return safely([&] { cavity::fdm_pass_noalloc(nx, ny, nz, s, st, inv_lambda, r, phi, (cudaStream_t)stream); });
+}
+int cavity_eigenbasis(const CavityConfig* config, int axis, int on_gpu, double* lambda, double* S) {
+    return safely([&] {
+        if (!config || axis < 0 || axis > 2 || !lambda || !S) throw std::runtime_error("cavity_eigenbasis: bad arguments");
+        const CavityConfig& c = *config;
+        const int n = axis == 0 ? c.nx : axis == 1 ? c.ny : c.nz;
+        if (n < 2) throw std::runtime_error("cavity_eigenbasis: an axis needs at least 2 cells");
+        const cavity::AxisGrid g = cavity::make_axis_grid(c, n, axis == 2 ? n * (c.lz / n) : c.length);
+        const cavity::AxisEigen e = on_gpu ? cavity::axis_eigen_gpu(g) : cavity::axis_eigen(g);
+        std::memcpy(lambda, e.lambda.data(), sizeof(double) * n);
+        std::memcpy(S, e.S.data(), sizeof(double) * n * n);
+    });
 }
 long long cavity_pressure_passes(const CavitySolver* s) { return s && s->s ? s->s->pressure_passes() : -1; }
 int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** out) {
