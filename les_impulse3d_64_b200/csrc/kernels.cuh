@@ -197,14 +197,16 @@ __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockI
 // values, stay fixed, and its column's values below and at the current layer carry over in registers.
 // blocks of a column kernel an SM is to hold: its loads run one layer ahead, so occupancy is its memory parallelism
 constexpr int kColumnBlocks = 4;
+constexpr int kResidualBlocks = 3;      // the residual's pairs of cells hold more in flight per thread
 struct ColumnSpan {
     int p, x, y, z0, z1;
     bool live;
 };
-__device__ __forceinline__ ColumnSpan column_span(const Params& p, const Blk& k) {
+// `per` consecutive cells of a row per thread (2: a pair starting at an even x; nx is even); s.p is the first
+__device__ __forceinline__ ColumnSpan column_span(const Params& p, const Blk& k, int per = 1) {
     ColumnSpan s;
     const int plane = p.nx * p.ny;
-    s.p = (int)k.x * kThreads + (int)threadIdx.x;
+    s.p = ((int)k.x * kThreads + (int)threadIdx.x) * per;
     s.live = s.p < plane;
     s.x = s.p % p.nx;
     s.y = s.p / p.nx;
@@ -574,27 +576,32 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     Vec<2> acc;
     acc.v[0] = 0.0;
     acc.v[1] = 0.0;
-    const ColumnSpan cs = column_span(p, k);
+    // a pair of cells (x, x + 1) per thread, x even: 16-byte loads and stores, and the pair's inner x-neighbours
+    // are its own values
+    const ColumnSpan cs = column_span(p, k, 2);
     if (!skip && cs.live && cs.z0 < cs.z1) {
         const int sy = p.nx, sz = p.nx * p.ny, x = cs.x, y = cs.y;
-        const double dx = a.dw[X][x], dy = a.dw[Y][y];
-        const bool xl = x > 0, xh = x + 1 < p.nx, yl = y > 0, yh = y + 1 < p.ny;
-        const double ixl = a.dinv_sp[X][x], ixh = a.dinv_sp[X][x + 1], iyl = a.dinv_sp[Y][y], iyh = a.dinv_sp[Y][y + 1];
+        const bool xl = x > 0, xh = x + 2 < p.nx, yl = y > 0, yh = y + 1 < p.ny;
         const double* f = a.phi;
+        const double* dwx = a.dw[X] + x;            // tables: L1 hits, read at use to keep registers for the loads
+        const double* ispx = a.dinv_sp[X] + x;
+        const double* ispy = a.dinv_sp[Y] + y;
+        auto ld2 = [](const double* q) { return __ldg(reinterpret_cast<const double2*>(q)); };
+        const double2 zero2 = make_double2(0.0, 0.0);
         // the loads of a layer that go to DRAM or to other blocks' rows, issued one layer ahead of its arithmetic;
-        // the same row's neighbours and the z tables are L1 hits by then
-        struct Layer { double above, n, s, rhs; };
+        // the same row's outer neighbours and the z tables are L1 hits by then
+        struct Layer { double2 above, n, s, rhs; };
         auto fetch = [&](int j, int z) {
             Layer v;
-            v.above = z + 1 < p.nz ? __ldg(f + j + sz) : 0.0;
-            v.n = yh ? __ldg(f + j + sy) : 0.0;
-            v.s = yl ? __ldg(f + j - sy) : 0.0;
-            v.rhs = __ldg(a.rhs + j);
+            v.above = z + 1 < p.nz ? ld2(f + j + sz) : zero2;
+            v.n = yh ? ld2(f + j + sy) : zero2;
+            v.s = yl ? ld2(f + j - sy) : zero2;
+            v.rhs = ld2(a.rhs + j);
             return v;
         };
         int i = cs.p + cs.z0 * sz;
-        double below = cs.z0 > 0 ? __ldg(f + i - sz) : 0.0;
-        double cc = __ldg(f + i);
+        double2 below = cs.z0 > 0 ? ld2(f + i - sz) : zero2;
+        double2 cc = ld2(f + i);
         Layer next = fetch(i, cs.z0);
         for (int z = cs.z0; z < cs.z1; z++, i += sz) {
             const Layer l = next;
@@ -605,17 +612,34 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
                 if (z + 2 + kColumnL2Ahead < p.nz) prefetch_l2(f + j + sz);
             }
             const double dz = __ldg(a.dw[Z] + z);
-            double s = 0.0;
-            if (xh) s += (dy * dz) * (__ldg(f + i + 1) - cc) * ixh;
-            if (xl) s -= (dy * dz) * (cc - __ldg(f + i - 1)) * ixl;
-            if (yh) s += (dx * dz) * (l.n - cc) * iyh;
-            if (yl) s -= (dx * dz) * (cc - l.s) * iyl;
-            if (z + 1 < p.nz) s += (dx * dy) * (l.above - cc) * __ldg(a.dinv_sp[Z] + z + 1);
-            if (z > 0) s -= (dx * dy) * (cc - below) * __ldg(a.dinv_sp[Z] + z);
-            const double r = l.rhs - s;
-            a.res[i] = r;
-            acc.v[0] += r * r;
-            acc.v[1] += cc;
+            const bool zh = z + 1 < p.nz;
+            const double izh = zh ? __ldg(a.dinv_sp[Z] + z + 1) : 0.0, izl = __ldg(a.dinv_sp[Z] + z);
+            const double west = xl ? __ldg(f + i - 1) : 0.0, east = xh ? __ldg(f + i + 2) : 0.0;
+            const double dx0 = __ldg(dwx), dx1 = __ldg(dwx + 1), dy = __ldg(a.dw[Y] + y);
+            const double ixl = __ldg(ispx), ixm = __ldg(ispx + 1), ixh = xh ? __ldg(ispx + 2) : 0.0;
+            const double iyl = __ldg(ispy), iyh = __ldg(ispy + 1);
+            // cell x (its east neighbour is the pair's other cell)
+            double s0 = 0.0;
+            s0 += (dy * dz) * (cc.y - cc.x) * ixm;
+            if (xl) s0 -= (dy * dz) * (cc.x - west) * ixl;
+            if (yh) s0 += (dx0 * dz) * (l.n.x - cc.x) * iyh;
+            if (yl) s0 -= (dx0 * dz) * (cc.x - l.s.x) * iyl;
+            if (zh) s0 += (dx0 * dy) * (l.above.x - cc.x) * izh;
+            if (z > 0) s0 -= (dx0 * dy) * (cc.x - below.x) * izl;
+            // cell x + 1 (its west neighbour is the pair's other cell)
+            double s1 = 0.0;
+            if (xh) s1 += (dy * dz) * (east - cc.y) * ixh;
+            s1 -= (dy * dz) * (cc.y - cc.x) * ixm;
+            if (yh) s1 += (dx1 * dz) * (l.n.y - cc.y) * iyh;
+            if (yl) s1 -= (dx1 * dz) * (cc.y - l.s.y) * iyl;
+            if (zh) s1 += (dx1 * dy) * (l.above.y - cc.y) * izh;
+            if (z > 0) s1 -= (dx1 * dy) * (cc.y - below.y) * izl;
+            const double r0 = l.rhs.x - s0, r1 = l.rhs.y - s1;
+            *reinterpret_cast<double2*>(a.res + i) = make_double2(r0, r1);
+            acc.v[0] += r0 * r0;
+            acc.v[0] += r1 * r1;
+            acc.v[1] += cc.x;
+            acc.v[1] += cc.y;
             below = cc;
             cc = l.above;
         }
@@ -652,8 +676,8 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
         }
     }
 }
-__global__ void __launch_bounds__(kThreads, kColumnBlocks) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
-__global__ void __launch_bounds__(kThreads, kColumnBlocks) residual_batched(const ResidualArgs* args) {
+__global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
+__global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_batched(const ResidualArgs* args) {
     __shared__ ResidualArgs a;
     int cav;
     const Blk k = batch_blk(1, cav);

@@ -726,8 +726,8 @@ private:
     // ------------------------------------------------------------------------------ kernel launches
     // grid of a column kernel (ColumnSpan): plane blocks along x and z-chunks along y, as many chunks as it takes
     // for the launch (all cavities of a batch together) to fill the device `per_sm` blocks deep
-    dim3 column_grid(int per_sm) const {
-        const long long bpp = blocks_for((long long)nx_ * ny_);
+    dim3 column_grid(int per_sm, int per_thread = 1) const {
+        const long long bpp = blocks_for((long long)nx_ * ny_ / per_thread);
         const long long want = (long long)sms_ * std::max(per_sm, 1);
         const long long cav = std::max(g_launch_batch, 1);
         long long chunks = std::min<long long>(nz_, std::max(1LL, want / (bpp * cav)));
@@ -808,7 +808,7 @@ private:
         a.partial = partial_;
         a.handle = h;
         a.use_handle = use_h;
-        const dim3 grid = column_grid(residual_per_sm_);
+        const dim3 grid = column_grid(residual_per_sm_, 2);     // a pair of cells per thread
         if (!record_launch(kLkResidual, 0, grid, 0, a)) check(launch_pdl(residual_kernel, grid, dim3(kThreads), 0, st, a));
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
