@@ -725,12 +725,17 @@ private:
 
     // ------------------------------------------------------------------------------ kernel launches
     // grid of a column kernel (ColumnSpan): plane blocks along x and z-chunks along y, as many chunks as it takes
-    // for the launch (all cavities of a batch together) to fill the device `per_sm` blocks deep
+    // for the launch (all cavities of a batch together) to fill the device `per_sm` blocks deep in one wave, or
+    // about four waves when the plane blocks alone exceed one
     dim3 column_grid(int per_sm, int per_thread = 1) const {
         const long long bpp = blocks_for((long long)nx_ * ny_ / per_thread);
         const long long want = (long long)sms_ * std::max(per_sm, 1);
         const long long cav = std::max(g_launch_batch, 1);
-        long long chunks = std::min<long long>(nz_, std::max(1LL, want / (bpp * cav)));
+        long long chunks = want / (bpp * cav);
+        // a launch that holds more plane blocks than fit at once (a large batch): chunks for about four waves, so
+        // that the last, partial wave is a small share of the launch
+        if (chunks < 1) chunks = (4 * want + bpp * cav - 1) / (bpp * cav);
+        chunks = std::min<long long>(nz_, std::max(1LL, chunks));
         const long long zc = (nz_ + chunks - 1) / chunks;
         chunks = (nz_ + zc - 1) / zc;
         return dim3((unsigned int)bpp, (unsigned int)chunks);
