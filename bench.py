@@ -183,8 +183,8 @@ def cell_kernel_bytes(settings, field_bytes):
             'finish': 2 * faces * field_bytes + 32 * cells}
 
 
-def cpu_oracle_rate(workload, steps_budget_s=12.0, max_steps=40):
-    """The FP64 OpenMP oracle on this host: cell-updates/s over a bounded number of steps."""
+def cpu_oracle_rate(workload, steps_budget_s=12.0, max_steps=40, warmup=1):
+    """The FP64 OpenMP oracle on this host: cell-updates/s over a bounded number of steps after `warmup`."""
     from les_impulse3d_64_b200 import workloads
     from les_impulse3d_64_b200.api import Solver
     sys.path.insert(0, str(ROOT / 'oracle'))
@@ -194,7 +194,8 @@ def cpu_oracle_rate(workload, steps_budget_s=12.0, max_steps=40):
     sim = Solver(w['settings'], library=ROOT / 'oracle' / 'libcavity_oracle.so')
     try:
         sim.initialize(*workloads.initial_noise(sim.shapes, w['noise'], w['seed']))
-        sim.step()                                    # warm-up (first-touch of the arrays)
+        for _ in range(max(1, warmup)):               # warm-up (first-touch of the arrays)
+            sim.step()
         t0 = time.perf_counter()
         n = 0
         while n < max_steps and (n < 2 or time.perf_counter() - t0 < steps_budget_s):
@@ -400,10 +401,12 @@ def run_serving(args, ranks):
 def run_reference(args, ranks):
     if ranks.rank != 0:
         return None
-    rate, n, dt = cpu_oracle_rate(args.workload, steps_budget_s=max(10.0, 2.0 * args.steps), max_steps=args.steps)
+    rate, n, dt = cpu_oracle_rate(args.workload, steps_budget_s=max(10.0, 2.0 * args.steps), max_steps=args.steps,
+                                  warmup=args.warmup)
     line = {
         'metric': 'cell-updates/s per RK3 step', 'value': rate, 'unit': 'cell-updates/s', 'n_gpus': ranks.world,
-        'steps': n, 'warmup': 1, 'ms_per_step': dt / n * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+        'steps': n, 'warmup': max(1, args.warmup), 'ms_per_step': dt / n * 1e3, 'higher_is_better': True,
+        'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded Gaussian initial noise, numpy default_rng)',
         'config': {'workload': args.workload}, 'impl': 'reference',
         'cpu_baseline': {'value': rate, 'unit': 'cell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
