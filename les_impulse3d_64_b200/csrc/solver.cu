@@ -845,8 +845,8 @@ private:
         if (!record_launch(kLkFinish, 0, grid, 0, a)) check(launch_pdl(finish_kernel<T>, grid, dim3(kThreads), 0, st, a));
     }
 
-    // A pressure refinement loop inside a stream capture: a conditional while-node whose body is one pass.
-    // `first_residual` launches the kernel that sets the loop condition before the node.
+    // A pressure refinement loop inside a stream capture: one pass, then a conditional while-node whose body is
+    // one pass.  `first_residual` launches the kernels that set the loop condition before them.
     template <class F>
     void captured_loop(F first_residual, double* phi) {
         cudaStreamCaptureStatus status;
@@ -857,6 +857,9 @@ private:
         cudaGraphConditionalHandle h;
         check(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
         first_residual(h);
+        // the first pass outside the loop: most solves need exactly one, and its kernels skip themselves when the
+        // start decided on none (the first transform clears the loop condition either way)
+        launch_pass(stream_, phi, h, 1);
         check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.type = cudaGraphNodeTypeConditional;
@@ -1181,6 +1184,8 @@ private:
                 check(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
             }
             emit(stream_, [&](S_& s) { s.launch_start(stream_, s.M_[out], true, stage, S, cur, h, 2); }, host, launch);
+            // the first pass outside the loop (see Solver::captured_loop), then the loop
+            emit(stream_, [&](S_& s) { s.launch_pass(stream_, s.praw_, h, 2); }, host, launch);
             if (launch) {
                 check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
                 cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
