@@ -106,9 +106,9 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 int cavity_kernel_times(CavitySolver* s, double* ms);
 /* The generalised eigenbasis of one axis's pressure operator, K S = W S diag(lambda) with S^T W S = I, for the grid
  * that `config` describes along `axis` (0 x, 1 y, 2 z): lambda[n] (the constant mode set to 0) and the row-major
- * n x n S, eigenvector j in column j.  on_gpu = 0: implicit-shift QL on the host; 1: bisection and inverse
- * iteration on the GPU (the default set-up of axes of 384 cells or more; CAVITY_EIGEN=host|gpu forces either in
- * solvers).  The eigenvectors' order and signs differ between the two.  The reference computes this basis by
+ * n x n S, eigenvector j in column j.  on_gpu = 0: implicit-shift QL on the host (the solvers' set-up); 1:
+ * bisection and inverse iteration on the GPU (the solvers' set-up with CAVITY_EIGEN=gpu).  The eigenvectors'
+ * order and signs differ between the two.  The reference computes this basis by
  * Jacobi rotations on the host (backend.cu:723-767); no counterpart of this function. */
 int cavity_eigenbasis(const CavityConfig* config, int axis, int on_gpu, double* lambda, double* S);
 /* The handle of the process-wide solver behind the solver_* functions (NULL if none). */

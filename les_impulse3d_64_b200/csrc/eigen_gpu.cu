@@ -1,4 +1,4 @@
-// eigen_gpu.cu - the pressure operator's 1-D eigenbases on the GPU (set-up of large grids).
+// eigen_gpu.cu - the pressure operator's 1-D eigenbases on the GPU (solver set-up with CAVITY_EIGEN=gpu).
 //
 // The generalised problem K S = W S diag(lambda) of an axis (backend.cu:723-767) is solved on its symmetric
 // tridiagonal form T = W^-1/2 K W^-1/2 (setup.cpp, axis_tridiagonal):
@@ -6,9 +6,10 @@
 //   - eigenvectors by inverse iteration on T - lambda I, factored by Gaussian elimination with partial pivoting
 //     (the tridiagonal LU of Golub and Van Loan, Matrix Computations, 4.3), three solves from a start vector
 //     with no symmetry (a symmetric one would miss the antisymmetric modes of a symmetric grid).
-// Eigenvalues closer than 1e-3 of the matrix norm form a cluster; one thread takes a cluster and orthogonalises
-// each of its vectors against the earlier ones after every solve (modified Gram-Schmidt), as the inverse
-// iteration of LAPACK's dstein does.  Work is O(n^2) in parallel, against O(n^3) in sequence for the host QL.
+// Eigenvalues closer than 1e-3 of the matrix norm form a cluster; one block takes a cluster and orthogonalises
+// each of its vectors against the earlier ones after every solve (Gram-Schmidt), as the inverse iteration of
+// LAPACK's dstein does.  On a stretched grid the low modes are closer than that, so one cluster can hold most of
+// the spectrum: its recurrences run on one thread and its projections on the whole block.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -57,81 +58,119 @@ __global__ void bisect_kernel(const double* d, const double* e2, int n, double l
     lambda[k] = 0.5 * (lo + hi);
 }
 
-// Inverse iteration for the eigenvalues of one cluster, [cluster[t], cluster[t + 1]), in thread t.  Workspace
-// `work`: 6 arrays of n per thread, element i of array a of thread t at (a * n + i) * threads + t (coalesced
-// across threads).  Eigenvector k goes to column k of the row-major Z.
-__global__ void inverse_iteration_kernel(const double* d, const double* e, int n, const double* lambda,
-                                         const int* cluster, int clusters, double tiny, double* work, double* Z) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= clusters) return;
-    const long long T = clusters;
-    auto at = [&](int a, int i) -> double& { return work[((long long)a * n + i) * T + t]; };
-    enum { kD = 0, kC, kC2, kL, kPiv, kB };
-    for (int k = cluster[t]; k < cluster[t + 1]; k++) {
+constexpr int kClusterThreads = 128;
+
+// sum over the block (every thread gets it)
+__device__ double block_sum(double v, double* red) {
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kClusterThreads / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// Inverse iteration for the eigenvalues of one cluster, [cluster[t], cluster[t + 1]), in block t (kClusterThreads
+// threads).  Thread 0 factors T - lambda I and solves with it (sequential recurrences, on the block's workspace,
+// which stays in L1); the block orthogonalises against the cluster's earlier vectors (classical Gram-Schmidt,
+// twice) and normalises.  Workspace `work`: 7 arrays of n per block.  Eigenvector k goes to column k of Z.
+__global__ void __launch_bounds__(kClusterThreads) inverse_iteration_kernel(const double* d, const double* e, int n,
+                                                                          const double* lambda, const int* cluster,
+                                                                          double tiny, double* work, double* Z) {
+    __shared__ double red[kClusterThreads];
+    const int t = blockIdx.x, tid = threadIdx.x;
+    double* D = work + (size_t)t * 7 * n;      // U: diagonal, superdiagonals C and C2; multipliers L; swaps P
+    double* C = D + n;
+    double* C2 = C + n;
+    double* L = C2 + n;
+    double* P = L + n;
+    double* B = P + n;                         // the iterate
+    double* G = B + n;                         // its projections on the cluster's earlier vectors
+    const int c0 = cluster[t], c1 = cluster[t + 1];
+    for (int k = c0; k < c1; k++) {
         const double lam = lambda[k];
-        // T - lam I = P L U: U with diagonal D, superdiagonals C and C2; multipliers L; row swaps Piv
-        for (int i = 0; i < n; i++) {
-            at(kD, i) = d[i] - lam;
-            at(kC, i) = i + 1 < n ? e[i] : 0.0;
-            at(kC2, i) = 0.0;
-        }
-        for (int i = 0; i + 1 < n; i++) {
-            const double sub = e[i];                       // below the diagonal in row i + 1
-            const double di = at(kD, i);
-            if (fabs(di) >= fabs(sub)) {
-                const double piv = di != 0.0 ? di : tiny;
-                at(kD, i) = piv;
-                const double m = sub / piv;
-                at(kL, i) = m;
-                at(kPiv, i) = 0.0;
-                at(kD, i + 1) -= m * at(kC, i);
-            } else {                                       // swap rows i and i + 1
-                const double m = di / sub;
-                at(kL, i) = m;
-                at(kPiv, i) = 1.0;
-                const double ci = at(kC, i), d1 = at(kD, i + 1), c1 = i + 2 < n ? at(kC, i + 1) : 0.0;
-                at(kD, i) = sub;
-                at(kC, i) = d1;
-                at(kC2, i) = c1;
-                at(kD, i + 1) = ci - m * d1;
-                if (i + 2 < n) at(kC, i + 1) = -m * c1;
+        if (tid == 0) {
+            for (int i = 0; i < n; i++) {
+                D[i] = d[i] - lam;
+                C[i] = i + 1 < n ? e[i] : 0.0;
+                C2[i] = 0.0;
             }
+            for (int i = 0; i + 1 < n; i++) {
+                const double sub = e[i];                   // below the diagonal in row i + 1
+                const double di = D[i];
+                if (fabs(di) >= fabs(sub)) {
+                    const double piv = di != 0.0 ? di : tiny;
+                    D[i] = piv;
+                    const double m = sub / piv;
+                    L[i] = m;
+                    P[i] = 0.0;
+                    D[i + 1] -= m * C[i];
+                } else {                                   // swap rows i and i + 1
+                    const double m = di / sub;
+                    L[i] = m;
+                    P[i] = 1.0;
+                    const double ci = C[i], d1 = D[i + 1], c1n = i + 2 < n ? C[i + 1] : 0.0;
+                    D[i] = sub;
+                    C[i] = d1;
+                    C2[i] = c1n;
+                    D[i + 1] = ci - m * d1;
+                    if (i + 2 < n) C[i + 1] = -m * c1n;
+                }
+            }
+            if (D[n - 1] == 0.0) D[n - 1] = tiny;
         }
-        if (at(kD, n - 1) == 0.0) at(kD, n - 1) = tiny;
         // start vector without symmetry, in (0.5, 1.5)
-        for (int i = 0; i < n; i++) {
+        for (int i = tid; i < n; i += kClusterThreads) {
             unsigned int h = (unsigned int)(i * 2654435761u) ^ (unsigned int)(k * 40503u + 12345u);
             h ^= h >> 13;
             h *= 0x5bd1e995u;
             h ^= h >> 15;
-            at(kB, i) = 0.5 + (double)(h & 0xffffff) / 16777216.0;
+            B[i] = 0.5 + (double)(h & 0xffffff) / 16777216.0;
         }
+        __syncthreads();
         for (int iter = 0; iter < 3; iter++) {
-            for (int i = 0; i + 1 < n; i++) {              // apply P and L
-                if (at(kPiv, i) != 0.0) {
-                    const double b0 = at(kB, i);
-                    at(kB, i) = at(kB, i + 1);
-                    at(kB, i + 1) = b0;
+            if (tid == 0) {
+                for (int i = 0; i + 1 < n; i++) {          // apply P and L
+                    if (P[i] != 0.0) {
+                        const double b0 = B[i];
+                        B[i] = B[i + 1];
+                        B[i + 1] = b0;
+                    }
+                    B[i + 1] -= L[i] * B[i];
                 }
-                at(kB, i + 1) -= at(kL, i) * at(kB, i);
+                for (int i = n - 1; i >= 0; i--) {        // back substitution with U
+                    double s = B[i];
+                    if (i + 1 < n) s -= C[i] * B[i + 1];
+                    if (i + 2 < n) s -= C2[i] * B[i + 2];
+                    B[i] = s / D[i];
+                }
             }
-            for (int i = n - 1; i >= 0; i--) {            // back substitution with U
-                double s = at(kB, i);
-                if (i + 1 < n) s -= at(kC, i) * at(kB, i + 1);
-                if (i + 2 < n) s -= at(kC2, i) * at(kB, i + 2);
-                at(kB, i) = s / at(kD, i);
+            __syncthreads();
+            for (int pass = 0; pass < 2 && k > c0; pass++) {   // orthogonal to the cluster's earlier vectors
+                for (int j = c0 + tid; j < k; j += kClusterThreads) {
+                    double s = 0.0;
+                    for (int i = 0; i < n; i++) s += Z[(long long)i * n + j] * B[i];
+                    G[j - c0] = s;
+                }
+                __syncthreads();
+                for (int i = tid; i < n; i += kClusterThreads) {
+                    double v = B[i];
+                    for (int j = c0; j < k; j++) v -= G[j - c0] * Z[(long long)i * n + j];
+                    B[i] = v;
+                }
+                __syncthreads();
             }
-            for (int j = cluster[t]; j < k; j++) {        // orthogonal to the cluster's earlier vectors
-                double dot = 0.0;
-                for (int i = 0; i < n; i++) dot += Z[(long long)i * n + j] * at(kB, i);
-                for (int i = 0; i < n; i++) at(kB, i) -= dot * Z[(long long)i * n + j];
-            }
-            double nrm = 0.0;
-            for (int i = 0; i < n; i++) nrm += at(kB, i) * at(kB, i);
-            const double inv = 1.0 / sqrt(nrm);
-            for (int i = 0; i < n; i++) at(kB, i) *= inv;
+            double part = 0.0;
+            for (int i = tid; i < n; i += kClusterThreads) part += B[i] * B[i];
+            const double inv = 1.0 / sqrt(block_sum(part, red));
+            for (int i = tid; i < n; i += kClusterThreads) B[i] *= inv;
+            __syncthreads();
         }
-        for (int i = 0; i < n; i++) Z[(long long)i * n + k] = at(kB, i);
+        for (int i = tid; i < n; i += kClusterThreads) Z[(long long)i * n + k] = B[i];
+        __syncthreads();
     }
 }
 
@@ -189,12 +228,12 @@ AxisEigen axis_eigen_gpu(const AxisGrid& g) {
     const int clusters = (int)cluster.size() - 1;
     if (err == cudaSuccess) {
         step(cudaMallocAsync((void**)&dc, sizeof(int) * cluster.size(), st));
-        step(cudaMallocAsync((void**)&dw, sizeof(double) * 6 * (size_t)n * clusters, st));
+        step(cudaMallocAsync((void**)&dw, sizeof(double) * 7 * (size_t)n * clusters, st));
     }
     if (err == cudaSuccess) {
         step(cudaMemcpyAsync(dc, cluster.data(), sizeof(int) * cluster.size(), cudaMemcpyHostToDevice, st));
-        inverse_iteration_kernel<<<(clusters + 63) / 64, 64, 0, st>>>(dd, de, n, dl, dc, clusters,
-                                                                      2.220446049250313e-16 * norm, dw, dz);
+        inverse_iteration_kernel<<<clusters, kClusterThreads, 0, st>>>(dd, de, n, dl, dc, 2.220446049250313e-16 * norm,
+                                                                       dw, dz);
         step(cudaGetLastError());
         step(cudaMemcpyAsync(Z.data(), dz, sizeof(double) * n * n, cudaMemcpyDeviceToHost, st));
         step(cudaStreamSynchronize(st));

@@ -5,6 +5,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 
 #include "layout.h"
@@ -180,11 +183,36 @@ AxisEigen axis_eigen_finish(const AxisGrid& g, std::vector<double> lambda, const
     return r;
 }
 
-bool eigen_on_gpu(int n) {
+namespace {
+// eigenbases already computed in this process, by the operator they belong to (widths and spacings of the axis,
+// compared exactly) and the solver that computed them; the oldest goes first beyond kEigenCacheEntries
+struct EigenEntry {
+    std::vector<double> width, spacing;
+    bool gpu;
+    std::shared_ptr<const AxisEigen> eigen;
+};
+constexpr size_t kEigenCacheEntries = 16;
+std::mutex g_eigen_mutex;
+std::deque<EigenEntry> g_eigen_cache;
+}  // namespace
+
+AxisEigen axis_eigen_shared(const AxisGrid& g) {
+    const bool gpu = eigen_on_gpu();
+    {
+        std::lock_guard<std::mutex> lock(g_eigen_mutex);
+        for (const EigenEntry& e : g_eigen_cache)
+            if (e.gpu == gpu && e.width == g.width && e.spacing == g.spacing) return *e.eigen;
+    }
+    auto eigen = std::make_shared<const AxisEigen>(gpu ? axis_eigen_gpu(g) : axis_eigen(g));
+    std::lock_guard<std::mutex> lock(g_eigen_mutex);
+    g_eigen_cache.push_back({g.width, g.spacing, gpu, eigen});
+    if (g_eigen_cache.size() > kEigenCacheEntries) g_eigen_cache.pop_front();
+    return *eigen;
+}
+
+bool eigen_on_gpu() {
     const char* m = std::getenv("CAVITY_EIGEN");
-    if (m && std::strcmp(m, "gpu") == 0) return true;
-    if (m && std::strcmp(m, "host") == 0) return false;
-    return n >= 384;
+    return m && std::strcmp(m, "gpu") == 0;
 }
 
 AxisEigen axis_eigen(const AxisGrid& g) {

@@ -32,8 +32,12 @@ void axis_tridiagonal(const AxisGrid& g, std::vector<double>& d, std::vector<dou
 AxisEigen axis_eigen_finish(const AxisGrid& g, std::vector<double> lambda, const std::vector<double>& Z);
 AxisEigen axis_eigen(const AxisGrid& g);
 AxisEigen axis_eigen_gpu(const AxisGrid& g);
-// the eigensolver of an axis of n cells: CAVITY_EIGEN=host or =gpu forces one, else the GPU from 384 cells
-bool eigen_on_gpu(int n);
+// the eigensolver of the solvers' set-up: the host QL, or the GPU solver when CAVITY_EIGEN=gpu (the host QL
+// measured faster at every size up to 512 cells)
+bool eigen_on_gpu();
+// The eigenbasis of an axis from the solver eigen_on_gpu picks, computed once per process for each operator:
+// cavities of the same size and stretching (ensembles, a serving stream) share it.  Thread-safe.
+AxisEigen axis_eigen_shared(const AxisGrid& g);
 
 // Largest viscous rate over cells, nu * sum over axes 4/(width * smaller spacing), in float as
 // backend.cu:1030-1034.

@@ -625,7 +625,7 @@ private:
         // pressure eigenbases (FP64) and 1/(lambda_x + lambda_y + lambda_z), 0 at the constant mode
         AxisEigen e[3];
         for (int a = 0; a < 3; a++) {
-            e[a] = eigen_on_gpu(ax_[a].n) ? axis_eigen_gpu(ax_[a]) : axis_eigen(ax_[a]);
+            e[a] = axis_eigen_shared(ax_[a]);
             const int n = ax_[a].n;
             std::vector<double> st((size_t)n * n);
             for (int i = 0; i < n; i++)

@@ -1,5 +1,5 @@
-"""The pressure operator's eigenbasis computed on the GPU (bisection and inverse iteration, the set-up of large
-axes) against the host's implicit-shift QL, and a solver set up with it against one set up on the host."""
+"""The pressure operator's eigenbasis computed on the GPU (bisection and inverse iteration, the set-up with
+CAVITY_EIGEN=gpu) against the host's implicit-shift QL, and a solver set up with it against one set up on the host."""
 import ctypes as ct
 
 import numpy as np
