@@ -217,7 +217,7 @@ __device__ __forceinline__ ColumnSpan column_span(const Params& p, const Blk& k,
 }
 // Layers of a column walk that are brought into L2 ahead of the one whose loads go out into registers: the L2
 // prefetch holds no register, so it deepens the walk's memory parallelism for free.
-constexpr int kColumnL2Ahead = 3;
+constexpr int kColumnL2Ahead = 1;
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 // Programmatic dependent launch: the step kernels are launched so that the next kernel may start while this one
 // finishes.  Every step kernel lets its dependents launch at entry and waits for its predecessor to complete
