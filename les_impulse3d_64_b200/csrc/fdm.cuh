@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_batched(cons
     dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, k, first_block());
 }
 
-// one batched transform launch; the tile shape keeps at least ~two CTAs per SM on small grids
+// one batched transform launch; the tile shape keeps at least ~two CTAs per SM on small grids.  The small tile runs
+// 8 warps (2 x 4, each 16 x 8) rather than 4: more warps hide the FP64 MMA chains of a latency-bound 64^3 pass.
 inline void launch_transform(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda,
                              long long sA, const double* B, int ldb, long long sB, double* C, int ldc, long long sC,
                              int batch, int epi, const double* inv_lambda, double* phi, const Control* c,
@@ -170,7 +171,7 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
         if (!record_launch(kLkDgemm64, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<64, 64, 2, 2, 32>, grid, dim3(128), 0, st, g);
     } else {
         dim3 grid((N + 31) / 32, (M + 31) / 32, batch);
-        if (!record_launch(kLkDgemm32, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<32, 32, 2, 2, 64>, grid, dim3(128), 0, st, g);
+        if (!record_launch(kLkDgemm32, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<32, 32, 2, 4, 64>, grid, dim3(256), 0, st, g);
     }
 }
 

@@ -1158,7 +1158,7 @@ private:
             check(launch_pdl(dgemm_mma_batched<64, 64, 2, 2, 32>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, per));
             break;
         case kLkDgemm32:
-            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 2, 64>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, per));
+            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 4, 64>, g, dim3(256), 0, st, (const GemmArgs<double>*)d, per));
             break;
         case kLkTc: launch_tc_batched(r.variant, g, per, (const TcTransformArgs*)d, st); break;
         default: fail("batch: unknown launch");
