@@ -233,6 +233,14 @@ def reference_gpu_rate(workload, steps, warmup):
 
 
 # ------------------------------------------------------------------------------------------ arms
+def workload_config(args, w, precision, world):
+    """The `config` of a bench line, the same dict in both arms."""
+    s = w['settings']
+    return {'workload': args.workload, 'grid': [s['nx'], s['ny'], s['nz']], 'precision': precision,
+            'stretch_beta': w.get('beta'), 're': round(1.0 / s['nu']),
+            'l2': 'GPU steps: flushed before each timed step (256 MiB write)', 'parallelism': f'replicas x{world}'}
+
+
 def run_ours(args, ranks):
     from les_impulse3d_64_b200 import _build, workloads
     from les_impulse3d_64_b200.api import Cavity, Solver
@@ -308,10 +316,8 @@ def run_ours(args, ranks):
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64' if precision == 'fp64' else 'f32',
         'data': 'synthetic (seeded Gaussian initial noise, numpy default_rng)',
-        'config': {'workload': args.workload, 'grid': [s['nx'], s['ny'], s['nz']], 'precision': precision,
-                   'stretch_beta': w.get('beta'), 're': round(1.0 / s['nu']),
-                   'l2': 'flushed before each timed step (256 MiB write)', 'parallelism': f'replicas x{ranks.world}',
-                   'device_bytes': device_bytes},
+        'config': workload_config(args, w, precision, ranks.world),
+        'device_bytes': device_bytes,
         'e2e': {'value': ranks.world * cells * args.steps / e2e_s, 'unit': 'cell-updates/s',
                 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
         'e2e_queued_outputs': {'value': ranks.world * cells * args.steps / queued_s, 'unit': 'cell-updates/s',
@@ -401,6 +407,8 @@ def run_serving(args, ranks):
 def run_reference(args, ranks):
     if ranks.rank != 0:
         return None
+    from les_impulse3d_64_b200 import workloads
+    w = workloads.WORKLOADS[args.workload]
     rate, n, dt = cpu_oracle_rate(args.workload, steps_budget_s=max(10.0, 2.0 * args.steps), max_steps=args.steps,
                                   warmup=args.warmup)
     line = {
@@ -408,7 +416,8 @@ def run_reference(args, ranks):
         'steps': n, 'warmup': max(1, args.warmup), 'ms_per_step': dt / n * 1e3, 'higher_is_better': True,
         'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic (seeded Gaussian initial noise, numpy default_rng)',
-        'config': {'workload': args.workload}, 'impl': 'reference',
+        'config': workload_config(args, w, args.precision or w.get('precision', 'fp64'), ranks.world),
+        'impl': 'reference',
         'cpu_baseline': {'value': rate, 'unit': 'cell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
                          'sample': f'{n} steps of {args.workload}, {dt:.1f} s (the reference ships no CPU path; '
                                    'this is its FP64 OpenMP restatement)'},

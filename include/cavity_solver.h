@@ -166,10 +166,12 @@ int cavity_fdm_pass_tf32(int nx, int ny, int nz, const double* const s[3], const
  * fail or a cudaFree would stall every stream.  Same arguments and result as cavity_fdm_pass; the caller
  * still passes every input and output.  The two intermediates live in a file-scope device array of
  * 2 x 262144 doubles (4 MiB, with a control block) that every GPU loading the library holds until the
- * process exits, so nx*ny*nz is limited to 262144 cells (64^3); larger grids are rejected with an error.
- * The first call on each device looks up the array's device address once (set-up); make that first call
- * before any stream capture.  All calls on a device share the array, which keeps the last call's contents:
- * each call resets the control flags that must start at zero, and calls that overlap on the GPU race. */
+ * process exits, so nx*ny*nz is limited to 262144 cells (64^3), and each axis to 1 <= n <= 1024 as for
+ * cavity_fdm_pass; other grids are rejected with an error.  The first call on each device looks up the
+ * array's device address once (set-up).  Every call is synchronous: it copies a control block from the
+ * host and waits for `stream`, so it must not be called on a stream that is being captured.  All calls on a
+ * device share the array, which keeps the last call's contents: each call resets the control flags that
+ * must start at zero, and calls that overlap on the GPU race. */
 int cavity_fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                             const double* inv_lambda, const double* r, double* phi, void* stream);
 /* Pressure passes run by this cavity since it was created (all stages, steps and projections). */

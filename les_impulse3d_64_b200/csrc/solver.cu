@@ -376,7 +376,25 @@ public:
     struct CkHeader {
         unsigned long long magic;
         int nx, ny, nz, field_bytes;
+        unsigned long long config_key;      // config_key(): the settings that decide how the state evolves
     };
+    // FNV-1a over the settings that decide the next steps (everything but the probe positions), field by
+    // field so that struct padding never enters it
+    unsigned long long config_key() const {
+        unsigned long long h = 1469598103934665603ull;
+        auto mix = [&](const void* p, size_t n) {
+            const unsigned char* b = static_cast<const unsigned char*>(p);
+            for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+        };
+        const int ints[] = {c_.nx, c_.ny, c_.nz, c_.lid_shaped, c_.impulse_order, c_.adaptive_dt, c_.dt_lag,
+                            c_.phi_extrapolate, c_.fdm_max_passes, c_.grid_stretch};
+        const double dbls[] = {c_.length, c_.u_lid, c_.nu, c_.lz, c_.lid_ramp_t, c_.reinit_r, c_.impulse_order4_ramp,
+                               c_.grid_dx_wall, c_.grid_max_aspect, c_.dt_fixed, c_.dt_max, c_.cfl_target,
+                               c_.diffusion_limit, c_.fdm_rtol};
+        mix(ints, sizeof ints);
+        mix(dbls, sizeof dbls);
+        return h;
+    }
     static constexpr unsigned long long kCkMagic = 0x43415654594b5031ull;
     struct CkLayout {
         size_t ctrl, u[3], m[3], phi, hist[4], stats, total;
@@ -400,7 +418,7 @@ public:
         const CkLayout L = ck_layout();
         const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
         char* d = static_cast<char*>(dst);
-        const CkHeader h{kCkMagic, nx_, ny_, nz_, (int)sizeof(T)};
+        const CkHeader h{kCkMagic, nx_, ny_, nz_, (int)sizeof(T), config_key()};
         check(cudaMemcpyAsync(d, &h, sizeof h, device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost, stream_));
         check(cudaMemcpyAsync(d + L.ctrl, ctrl_, sizeof(Control), kind, stream_));
         for (int k = 0; k < 3; k++) {
@@ -422,6 +440,8 @@ public:
         if (h.magic != kCkMagic) fail("checkpoint: not a cavity checkpoint");
         if (h.nx != nx_ || h.ny != ny_ || h.nz != nz_ || h.field_bytes != (int)sizeof(T))
             fail("checkpoint: grid size or precision form differs from this solver");
+        if (h.config_key != config_key())
+            fail("checkpoint: saved by a solver with other settings (stretching, Re, lid, dt or solver options)");
         check(cudaMemcpyAsync(ctrl_, d + L.ctrl, sizeof(Control), kind, stream_));
         for (int k = 0; k < 3; k++) {
             check(cudaMemcpyAsync(U_[par_][k], d + L.u[k], sizeof(T) * size_[k], kind, stream_));
@@ -1366,7 +1386,8 @@ static NoAllocScratch noalloc_scratch() {
 
 static void fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], const double* const st[3],
                              const double* inv_lambda, const double* r, double* phi, cudaStream_t stream) {
-    if (nx < 1 || ny < 1 || nz < 1) fail("fdm pass (no allocation): nx, ny, nz must be >= 1");
+    if (nx < 1 || ny < 1 || nz < 1 || nx > 1024 || ny > 1024 || nz > 1024)
+        fail("fdm pass (no allocation): 1 <= nx, ny, nz <= 1024");
     const long long n = (long long)nx * ny * nz;
     if (n > kNoAllocMaxCells) {
         char msg[200];

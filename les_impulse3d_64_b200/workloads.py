@@ -78,6 +78,45 @@ def kick_noise(shapes, seed, number):
     return [rng.standard_normal(shapes[c]) for c in 'uvw']
 
 
+def run_protocol(sim, workload, steps=None, snapshots=(), on_snapshot=None):
+    """Drive a solver through a workload's run, step by step, in the order of the reference's run script
+    (main.py:342-363): one step, then the probes, then a kick if one is due, then the statistics.
+
+    Kicks and the statistics window are indexed by step number (the configs give them so; main.py keys them
+    on time): kick (n, amp) follows step n, and every step n > stats_from adds the mid-span field with weight
+    dt.  `sim` is any binding of the solver ABI (the B200 build, the oracle, the reference).
+    `on_snapshot(n, sim)` is called after step n for every n in `snapshots`.
+
+    Returns per-step arrays: dt, time, dt_reason, phi_passes, probes (steps x 2 n_probes, float32), the KE
+    before and after each kick, and the centreline samples of the statistics steps."""
+    steps = workload['steps'] if steps is None else steps
+    kicks = dict(workload.get('kicks', ()))
+    stats_from = workload.get('stats_from')
+    out = dict(dt=[], time=[], dt_reason=[], phi_passes=[], probes=[], kick_ke=[], centreline=[])
+    for n in range(1, steps + 1):
+        rep = sim.step()
+        out['dt'].append(rep['dt'])
+        out['time'].append(rep['time'])
+        out['dt_reason'].append(rep['dt_reason'])
+        out['phi_passes'].append(rep['phi_passes'])
+        out['probes'].append(sim.probes())
+        if n in kicks:
+            before = sim.diagnostics()['kinetic_energy']
+            sim.kick(kick_noise(sim.shapes, workload['seed'], sorted(kicks).index(n) + 1), kicks[n], KICK_PASSES)
+            out['kick_ke'].append((before, sim.diagnostics()['kinetic_energy']))
+        if stats_from is not None and n > stats_from:
+            out['centreline'].append(sim.add_statistics(rep['dt']))
+        if n in snapshots and on_snapshot is not None:
+            on_snapshot(n, sim)
+    res = {k: np.asarray(v) for k, v in out.items()}
+    res['dt_reason'] = np.asarray(out['dt_reason'], dtype=object)
+    return res
+
+
+# smoothing passes of a kick: KICK_CELLS // 2 with the run script's 20-cell eddies (main.py:54, 356)
+KICK_PASSES = 10
+
+
 def ensemble_cases(count=256, seed=0, sizes=(24, 32, 48, 64), re_range=(100.0, 2000.0), noise=1e-3):
     """C4: `count` cavities, sizes drawn uniformly from `sizes`, half uniform and half stretched (beta 1.5),
     Re log-uniform in `re_range`, independent noise seeds; mixed form, CFL 0.5."""

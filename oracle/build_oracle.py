@@ -22,7 +22,8 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REFERENCE_SOURCE = Path('/root/reference/backend.cu')
+# the reference checkout: CAVITY_REFERENCE_DIR, by default where this machine keeps it
+REFERENCE_SOURCE = Path(os.environ.get('CAVITY_REFERENCE_DIR', '/root/reference')) / 'backend.cu'
 CUDA_HOME = Path(os.environ.get('CUDA_HOME', '/usr/local/cuda'))
 
 

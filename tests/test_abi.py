@@ -1,6 +1,7 @@
 """The C ABI without a GPU: every symbol include/cavity_solver.h declares is exported by the built library,
 the record layouts match the reference's (byte sizes and offsets), and calls without a solver fail cleanly."""
 import ctypes as ct
+import os
 import re
 from pathlib import Path
 
@@ -37,19 +38,21 @@ def test_record_layouts():
     assert ct.sizeof(Report) == 48 and ct.sizeof(Diagnostics) == 64
 
 
+def _our_layouts():
+    return {name: {'size': ct.sizeof(rec), 'fields': [[n, getattr(rec, n).offset] for n, _ in rec._fields_]}
+            for name, rec in (('Config', Config), ('Report', Report), ('Diagnostics', Diagnostics))}
+
+
 def test_layouts_match_reference_binding():
-    """The reference's own python_api records, where its checkout is present."""
-    import importlib.util
-    src = Path('/root/reference/python_api.py')
-    if not src.is_file():
-        pytest.skip('reference checkout not present')
-    spec = importlib.util.spec_from_file_location('reference_python_api', src)
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    for ours, theirs in ((Config, mod.Config), (Report, mod.Report), (Diagnostics, mod.Diagnostics)):
-        assert ct.sizeof(ours) == ct.sizeof(theirs)
-        assert [(n, getattr(ours, n).offset) for n, _ in ours._fields_] == \
-               [(n, getattr(theirs, n).offset) for n, _ in theirs._fields_]
+    """The reference's own python_api records (python_api.py:11-28), as recorded in
+    tests/golden/record_layouts.json by tests/golden/make_layouts.py; and, when CAVITY_REFERENCE_DIR names a
+    reference checkout, read live from it as well."""
+    import json
+    assert _our_layouts() == json.loads((ROOT / 'tests' / 'golden' / 'record_layouts.json').read_text())
+    folder = os.environ.get('CAVITY_REFERENCE_DIR')
+    if folder and (Path(folder) / 'python_api.py').is_file():
+        from make_layouts import layouts
+        assert _our_layouts() == layouts(Path(folder) / 'python_api.py')
 
 
 def test_calls_without_solver_fail_with_message(lib):

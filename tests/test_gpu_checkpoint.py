@@ -70,3 +70,25 @@ def test_checkpoint_rejects_another_grid():
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize('change', [dict(beta=2.0), dict(re=2000.0), dict(lid='uniform'), dict(impulse_order=2)])
+def test_checkpoint_rejects_other_settings(change):
+    """Same grid size and precision, but another stretching, Re, lid or impulse order: the saved dt lag,
+    CFL state and potential history belong to another run, so the load is refused."""
+    base = dict(beta=1.5, re=1000.0, lid='regularised', impulse_order=4)
+    other = dict(base, **change)
+    a = Cavity(workloads.settings(16, base['re'], beta=base['beta'], lid=base['lid'],
+                                  impulse_order=base['impulse_order']), precision='fp64')
+    b = Cavity(workloads.settings(16, other['re'], beta=other['beta'], lid=other['lid'],
+                                  impulse_order=other['impulse_order']), precision='fp64')
+    try:
+        a.initialize()
+        ck = a.checkpoint()
+        with pytest.raises(RuntimeError, match='other settings'):
+            b.restore(ck)
+        b.initialize()
+        b.restore(b.checkpoint())      # its own checkpoint still loads
+    finally:
+        a.close()
+        b.close()

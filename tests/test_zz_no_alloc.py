@@ -21,10 +21,12 @@ def _fn(lib, name):
     return fn
 
 
-def test_noalloc_pass_matches_allocating_pass_twice():
+@pytest.mark.parametrize('shape', [(40, 40, 33), (64, 64, 64)])
+def test_noalloc_pass_matches_allocating_pass_twice(shape):
+    """A ragged grid, and 64^3, the full size of the shared device array."""
     lib = load_library()
     lib.cavity_last_error.restype = ct.c_char_p
-    S, il, r, phi = random_operands(40, 40, 33, seed=11)
+    S, il, r, phi = random_operands(*shape, seed=11)
     nz, ny, nx = r.shape
     ds = [device(s) for s in S]
     dst = [device(s.T.copy()) for s in S]
@@ -40,10 +42,16 @@ def test_noalloc_pass_matches_allocating_pass_twice():
         assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), f'call {call + 1}'
 
 
-def test_noalloc_pass_rejects_grids_beyond_its_limit():
+@pytest.mark.parametrize('shape, message', [((65, 64, 64), b'exceeds the maximum of 262144'),
+                                            ((2048, 64, 1), b'1 <= nx, ny, nz <= 1024'),
+                                            ((2, 2, 65536), b'1 <= nx, ny, nz <= 1024'),
+                                            ((0, 8, 8), b'1 <= nx, ny, nz <= 1024')])
+def test_noalloc_pass_rejects_grids_beyond_its_limit(shape, message):
+    """Over the cell limit, or one axis over 1024 cells with fewer than 262144 cells in all: rejected with a
+    message before anything is launched (the pointers here are never dereferenced)."""
     lib = load_library()
     lib.cavity_last_error.restype = ct.c_char_p
     sp = (ct.c_void_p * 3)(1, 1, 1)
-    rc = _fn(lib, 'cavity_fdm_pass_noalloc')(65, 64, 64, sp, sp, 1, 1, 1, None)
+    rc = _fn(lib, 'cavity_fdm_pass_noalloc')(*shape, sp, sp, 1, 1, 1, None)
     assert rc == 1
-    assert b'exceeds the maximum of 262144' in lib.cavity_last_error()
+    assert message in lib.cavity_last_error()
