@@ -40,6 +40,8 @@ def parse_args():
     ap.add_argument('--workload', default='c2_64cube_re1000')
     ap.add_argument('--precision', choices=('fp64', 'mixed'), default=None)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-batched', action='store_true',
+                    help='skip the batched mixed-form sub-measurements of the default line')
     ap.add_argument('--count', type=int, default=256, help='cavities of the c4_ensemble workload')
     ap.add_argument('--chunk', type=int, default=8, help='steps queued per cavity between waits (ensemble)')
     ap.add_argument('--requests', type=int, default=64, help='requests of the c5_serving stream')
@@ -241,6 +243,28 @@ def workload_config(args, w, precision, world):
             'l2': 'GPU steps: flushed before each timed step (256 MiB write)', 'parallelism': f'replicas x{world}'}
 
 
+def batched_rates(steps, warmup, chunk=8):
+    """Sub-measurements of the default line: the mixed form batched (wall clock over all cavities, steps queued
+    `chunk` at a time): 64 cavities of the C2 cavity (64^3, beta 1.5, Re 1000; seeds 0..63), and the C4 ensemble
+    (256 cavities of 24^3..64^3)."""
+    from les_impulse3d_64_b200 import workloads
+    from les_impulse3d_64_b200.ensemble import Ensemble
+    c2 = workloads.C2
+    out = {}
+    for name, cases in (('batched_mixed_64cube',
+                         [dict(name=f'c2_{k}', settings=c2['settings'], noise=c2['noise'], seed=k, precision='mixed')
+                          for k in range(64)]),
+                        ('c4_ensemble_mixed', workloads.ensemble_cases(count=256))):
+        ens = Ensemble(cases)
+        try:
+            dt, rate = ens.timed(steps, warmup=warmup, chunk=chunk)
+            out[name] = {'value': rate, 'unit': 'cell-updates/s', 'cavities': len(cases), 'cells': sum(ens.cells),
+                         'steps': steps, 'seconds': dt, 'timing': 'wall clock over all cavity streams'}
+        finally:
+            ens.close()
+    return out
+
+
 def run_ours(args, ranks):
     from les_impulse3d_64_b200 import _build, workloads
     from les_impulse3d_64_b200.api import Cavity, Solver
@@ -330,6 +354,14 @@ def run_ours(args, ranks):
         'stencil_kernels': cell_kernels,
         'clocks': clocks.summary(),
     }
+    if not args.no_batched and args.workload == 'c2_64cube_re1000':
+        # the mixed form batched against this line's plain FP64 value (device time, single cavity)
+        ranks.barrier()
+        sub = batched_rates(args.steps, max(3, args.warmup))
+        for v in sub.values():
+            v['value'] = ranks.world * v['value'] * (v['seconds'] / ranks.max(v['seconds']))
+            v['ratio_vs_value'] = v['value'] / value
+        line['batched'] = sub
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
         rate, n, dt = cpu_oracle_rate(args.workload)
         line['cpu_baseline'] = {'value': rate, 'unit': 'cell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',

@@ -304,6 +304,16 @@ class Cavity:
                    pointer(kms))
         return ms, kms
 
+    def autotune(self, steps=6):
+        """Pick the fastest launch shapes for this cavity by timing `steps` steps per candidate (state restored);
+        returns (march z-chunks, FP64 transform tile, one-launch pass, ms per step).  See cavity_autotune."""
+        L = self.lib
+        L.cavity_autotune.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+        chunks, tile, fused, ms = ct.c_int(0), ct.c_int(0), ct.c_int(0), ct.c_float(0)
+        self._call('cavity_autotune', self.handle, int(steps), ct.byref(chunks), ct.byref(tile), ct.byref(fused),
+                   ct.byref(ms))
+        return chunks.value, tile.value, fused.value, ms.value
+
     def kernel_times(self):
         """Mean device time per step (ms, three stages) of the sweeps, projection starts, residuals of their
         guesses and finishes, over the last `time_steps` call."""

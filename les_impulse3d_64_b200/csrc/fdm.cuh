@@ -3,6 +3,8 @@
 // phi += S_x S_y S_z t.  Fields are [z][y][x]; S_a is the row-major n_a x n_a eigenbasis of axis a
 // (eigenvector j in column j) and ST_a its transpose.
 #pragma once
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "kernels.cuh"
@@ -138,23 +140,77 @@ template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
 __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_kernel(GemmArgs<double> g) {
     dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, real_blk(), first_block());
 }
-// a batch of cavities: grid z runs over cavities x `per` transform batches
+// a batch of cavities: grid x runs over the work list (BatchItem)
 template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
 __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_batched(const GemmArgs<double>* args,
-                                                                            unsigned int per) {
+                                                                            const BatchItem* items) {
     __shared__ GemmArgs<double> g;
     int cav;
-    const Blk k = batch_blk(per, cav);
+    const Blk k = item_blk(items, cav);
     load_args(g, args + cav);
     dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, k, first_block());
 }
 
+// ---------------------------------------------------------------------------------------------- one-launch pass
+// The six transforms of a pass as phases of one cooperative launch, separated by grid barriers: a small grid's
+// transforms are each a few microseconds of latency-bound work, and one launch replaces six.  Each phase runs
+// the same 32 x 32 tile body over that transform's own tile grid (grid-stride), so the arithmetic is exactly
+// that of six launches.  Every barrier wait is bounded: on time-out the block sets kBarrierWait and returns.
+struct FdmPassArgs {
+    GemmArgs<double> g[6];
+    unsigned int gx[6], gy[6], gz[6];      // each transform's tile grid
+    Control* c;
+};
+constexpr long long kBarrierSpins = 1LL << 22;
+
+// all blocks of the launch (co-resident: cooperative launch) meet here; false if the wait timed out
+__device__ __forceinline__ bool grid_barrier(Control* c, unsigned int nblocks) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = &c->counter[kCntBarGen];
+        const unsigned int g0 = *gen;
+        ok = 1;
+        __threadfence();
+        if (atomicAdd(&c->counter[kCntBar], 1u) == nblocks - 1) {
+            atomicExch(&c->counter[kCntBar], 0u);
+            __threadfence();
+            atomicAdd(&c->counter[kCntBarGen], 1u);
+        } else {
+            long long spins = 0;
+            while (*gen == g0) {
+                if (++spins > kBarrierSpins) {
+                    atomicExch(&c->error, (int)kBarrierWait);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok;
+}
+
+__global__ void __launch_bounds__(256) fdm_pass_fused_kernel(FdmPassArgs a) {
+    const unsigned int nb = gridDim.x;
+    for (int p = 0; p < 6; p++) {
+        const unsigned int tiles = a.gx[p] * a.gy[p] * a.gz[p];
+        for (unsigned int vb = blockIdx.x; vb < tiles; vb += nb) {
+            const Blk k{vb % a.gx[p], (vb / a.gx[p]) % a.gy[p], vb / (a.gx[p] * a.gy[p]), a.gx[p], a.gy[p], a.gz[p]};
+            dgemm_mma_body<32, 32, 2, 4, 64>(a.g[p], k, p == 0 && vb == 0);
+        }
+        if (p < 5 && !grid_barrier(a.c, nb)) return;
+    }
+}
+
 // one batched transform launch; the tile shape keeps at least ~two CTAs per SM on small grids.  The small tile runs
 // 8 warps (2 x 4, each 16 x 8) rather than 4: more warps hide the FP64 MMA chains of a latency-bound 64^3 pass.
-inline void launch_transform(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda,
-                             long long sA, const double* B, int ldb, long long sB, double* C, int ldc, long long sC,
-                             int batch, int epi, const double* inv_lambda, double* phi, const Control* c,
-                             cudaGraphConditionalHandle h, bool clear) {
+inline GemmArgs<double> transform_args(int M, int N, int K, const double* A, const double* A_alt, int lda, long long sA,
+                                       const double* B, int ldb, long long sB, double* C, int ldc, long long sC, int epi,
+                                       const double* inv_lambda, double* phi, const Control* c,
+                                       cudaGraphConditionalHandle h, bool clear) {
     GemmArgs<double> g;
     g.handle = h;
     g.clear_condition = clear;
@@ -165,8 +221,16 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
     g.phi = phi;
     g.epilogue = epi;
     g.c = c;
+    return g;
+}
+inline void launch_transform(cudaStream_t st, int M, int N, int K, const double* A, const double* A_alt, int lda,
+                             long long sA, const double* B, int ldb, long long sB, double* C, int ldc, long long sC,
+                             int batch, int epi, const double* inv_lambda, double* phi, const Control* c,
+                             cudaGraphConditionalHandle h, bool clear) {
+    const GemmArgs<double> g = transform_args(M, N, K, A, A_alt, lda, sA, B, ldb, sB, C, ldc, sC, epi, inv_lambda, phi,
+                                              c, h, clear);
     const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch * g_launch_batch;
-    if (tiles64 >= 296) {
+    if (g_dgemm_tile ? g_dgemm_tile == 64 : tiles64 >= 296) {
         dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
         if (!record_launch(kLkDgemm64, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<64, 64, 2, 2, 32>, grid, dim3(128), 0, st, g);
     } else {
@@ -177,8 +241,76 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
 
 // phi += FDM(r); r_alt replaces r when the control block says use_rhs.  t1, t2: nx*ny*nz doubles of scratch.
 // `clear` makes the first launch clear the condition of the enclosing graph while-node `h`.
+// cooperative blocks of the one-launch pass this device holds at once (0: not available)
+inline int fused_pass_capacity() {
+    static const int cap = [] {
+        int dev = 0, sms = 0, per = 0, coop = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fdm_pass_fused_kernel, 256, 0) == cudaSuccess)
+            return sms * per;
+        return 0;
+    }();
+    return cap;
+}
+// One-launch pass: the six transforms of launch_fdm_pass with the 32 x 32 tile, as one cooperative launch.
+inline void launch_fdm_pass_fused(cudaStream_t st, const FdmOperands& op, const double* r, const double* r_alt,
+                                  double* phi, double* t1, double* t2, Control* c, cudaGraphConditionalHandle h,
+                                  bool clear) {
+    const int nx = op.nx, ny = op.ny, nz = op.nz, plane = nx * ny;
+    const long long pl = plane;
+    const double* il = op.inv_lambda;
+    FdmPassArgs a;
+    a.c = c;
+    struct Shape { int M, N, batch; };
+    const Shape sh[6] = {{ny * nz, nx, 1}, {ny, nx, nz}, {nz, plane, 1}, {nz, plane, 1}, {ny, nx, nz}, {ny * nz, nx, 1}};
+    a.g[0] = transform_args(ny * nz, nx, nx, r, r_alt, nx, 0, op.s[0], nx, 0, t1, nx, 0, kStore, il, nullptr, c, h, clear);
+    a.g[1] = transform_args(ny, nx, ny, op.st[1], nullptr, ny, 0, t1, nx, pl, t2, nx, pl, kStore, il, nullptr, c, 0, false);
+    a.g[2] = transform_args(nz, plane, nz, op.st[2], nullptr, nz, 0, t2, plane, 0, t1, plane, 0, kScaleInvLambda, il,
+                            nullptr, c, 0, false);
+    a.g[3] = transform_args(nz, plane, nz, op.s[2], nullptr, nz, 0, t1, plane, 0, t2, plane, 0, kStore, il, nullptr, c, 0,
+                            false);
+    a.g[4] = transform_args(ny, nx, ny, op.s[1], nullptr, ny, 0, t2, nx, pl, t1, nx, pl, kStore, il, nullptr, c, 0, false);
+    a.g[5] = transform_args(ny * nz, nx, nx, t1, nullptr, nx, 0, op.st[0], nx, 0, nullptr, nx, 0, kAccumulate, il, phi, c,
+                            0, false);
+    unsigned int most = 0;
+    for (int p = 0; p < 6; p++) {
+        a.gx[p] = (unsigned int)((sh[p].N + 31) / 32);
+        a.gy[p] = (unsigned int)((sh[p].M + 31) / 32);
+        a.gz[p] = (unsigned int)sh[p].batch;
+        most = std::max(most, a.gx[p] * a.gy[p] * a.gz[p]);
+    }
+    const unsigned int blocks = std::min(most, (unsigned int)fused_pass_capacity());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, fdm_pass_fused_kernel, a);
+}
+// the one-launch pass applies: a single cavity (not recording a batch) whose largest transform has at most two
+// tiles per co-resident block, unless CAVITY_FDM_FUSED says otherwise (=1 always, =0 never); `want` is the
+// cavity's own choice (autotuner): -1 by the rule
+inline bool use_fused_pass(const FdmOperands& op, int want) {
+    if (g_launch_record || g_dgemm_tile == 64 || fused_pass_capacity() == 0) return false;
+    if (const char* e = std::getenv("CAVITY_FDM_FUSED")) return e[0] == '1';
+    if (want >= 0) return want == 1;
+    const long long most = std::max({(long long)((op.nx + 31) / 32) * ((op.ny * op.nz + 31) / 32),
+                                     (long long)((op.nx + 31) / 32) * ((op.ny + 31) / 32) * op.nz,
+                                     (long long)((op.nx * op.ny + 31) / 32) * ((op.nz + 31) / 32)});
+    return most <= 2LL * fused_pass_capacity();
+}
+
 inline void launch_fdm_pass(cudaStream_t st, const FdmOperands& op, const double* r, const double* r_alt, double* phi,
-                            double* t1, double* t2, const Control* c, cudaGraphConditionalHandle h, bool clear) {
+                            double* t1, double* t2, Control* c, cudaGraphConditionalHandle h, bool clear, int fused = -1) {
+    if (use_fused_pass(op, fused)) {
+        launch_fdm_pass_fused(st, op, r, r_alt, phi, t1, t2, c, h, clear);
+        return;
+    }
     const int nx = op.nx, ny = op.ny, nz = op.nz, plane = nx * ny;
     const long long pl = plane;
     const double* il = op.inv_lambda;

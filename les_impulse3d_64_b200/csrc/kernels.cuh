@@ -29,6 +29,7 @@ namespace cavity {
 // launch (kind, template variant, grid, dynamic shared memory and argument record) to it instead of launching:
 // a batch of cavities collects every member's arguments for the same launch sequence this way and issues one
 // batched launch per entry.
+enum SweepKind : int { kSweepFace = 0, kSweepTile = 1, kSweepMarch = 2 };
 enum LaunchKind : int { kLkStepBegin = 0, kLkSweep, kLkStart, kLkResidual, kLkFinish, kLkDgemm64, kLkDgemm32, kLkTc };
 struct LaunchRecord {
     int kind, variant;
@@ -39,6 +40,8 @@ struct LaunchRecord {
 inline thread_local std::vector<LaunchRecord>* g_launch_record = nullptr;
 // number of cavities the recorded launches will cover: tile choices that depend on the size of the grid use it
 inline thread_local int g_launch_batch = 1;
+// FP64 transform tile forced for every cavity of a batch whose cavities differ in size (0: chosen by size)
+inline thread_local int g_dgemm_tile = 0;
 // launch a step kernel with programmatic stream serialization (see pdl_wait); inside a stream capture this makes
 // the graph edge to the previous kernel a programmatic one
 template <class... KArgs, class... Args>
@@ -74,8 +77,10 @@ enum ErrorCode : int {
     kResidualNaN = 3,      // backend.cu:838
     kNotConverged = 4,     // backend.cu:840-844
     kDeviceWait = 5,       // a bounded wait on the tensor cores ran out (no counterpart in the reference)
+    kBarrierWait = 6,      // a bounded grid-barrier wait of the one-launch FDM pass ran out (no counterpart)
 };
-enum Counter : int { kCntDiv = 0, kCntRes, kCntFinish, kCntCfl, kNumCounters };
+// arrival counters of the last-block reductions, and the grid barrier's arrival count and generation
+enum Counter : int { kCntDiv = 0, kCntRes, kCntFinish, kCntCfl, kCntBar, kCntBarGen, kNumCounters };
 
 struct alignas(16) Control {
     // clock, committed by the last stage of a successful step (backend.cu:945-954)
@@ -187,9 +192,15 @@ struct Blk {
     unsigned int x, y, z, nx, ny, nz;
 };
 __device__ __forceinline__ Blk real_blk() { return {blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y, gridDim.z}; }
-__device__ __forceinline__ Blk batch_blk(unsigned int per, int& cavity) {
-    cavity = (int)(blockIdx.z / per);
-    return {blockIdx.x, blockIdx.y, blockIdx.z % per, gridDim.x, gridDim.y, per};
+// A batched launch runs a work list: one entry per block, naming the cavity and the block's place in that
+// cavity's own launch grid, so cavities of different sizes share a launch (grid x runs over the list).
+struct BatchItem {
+    unsigned int cav, x, y, z, nx, ny, nz, pad;
+};
+__device__ __forceinline__ Blk item_blk(const BatchItem* items, int& cavity) {
+    const BatchItem it = items[blockIdx.x];
+    cavity = (int)it.cav;
+    return {it.x, it.y, it.z, it.nx, it.ny, it.nz};
 }
 __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0; }
 // Cells visited as columns: a block takes kThreads consecutive cells of an x-y plane (x fastest) and walks them
@@ -538,10 +549,10 @@ __global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_kern
     projection_start_body(a, real_blk());
 }
 template <class T>
-__global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_batched(const StartArgs<T>* args) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_batched(const StartArgs<T>* args, const BatchItem* items) {
     __shared__ StartArgs<T> a;
     int cav;
-    const Blk k = batch_blk(1, cav);
+    const Blk k = item_blk(items, cav);
     load_args(a, args + cav);
     projection_start_body(a, k);
 }
@@ -677,10 +688,10 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     }
 }
 __global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
-__global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_batched(const ResidualArgs* args) {
+__global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_batched(const ResidualArgs* args, const BatchItem* items) {
     __shared__ ResidualArgs a;
     int cav;
-    const Blk k = batch_blk(1, cav);
+    const Blk k = item_blk(items, cav);
     load_args(a, args + cav);
     residual_body(a, k);
 }
@@ -860,10 +871,10 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
 template <class T>
 __global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_kernel(FinishArgs<T> a) { finish_body(a, real_blk()); }
 template <class T>
-__global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_batched(const FinishArgs<T>* args) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_batched(const FinishArgs<T>* args, const BatchItem* items) {
     __shared__ FinishArgs<T> a;
     int cav;
-    const Blk k = batch_blk(1, cav);
+    const Blk k = item_blk(items, cav);
     load_args(a, args + cav);
     finish_body(a, k);
 }

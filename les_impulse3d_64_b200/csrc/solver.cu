@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -25,6 +26,7 @@
 #include "fdm.cuh"
 #include "tc_gemm.cuh"
 #include "sweep.cuh"
+#include "sweep_march.cuh"
 #include "sweep_tile.cuh"
 #include "outputs.cuh"
 #include "setup.h"
@@ -84,6 +86,63 @@ private:
 
 static long long estimate_bytes(const CavityConfig& c, int precision);
 
+// ------------------------------------------------------------------------------------------ autotuner cache
+// Launch shapes chosen by timing (Solver::autotune), per grid size, stretching and precision form: the z-chunk
+// count of the march sweep and the FP64 transform tile.  Neither changes the arithmetic of a step.  Kept for the
+// process and, when CAVITY_TUNE_FILE names a file, read from it once and appended to it.
+struct Tuning {
+    int chunks = 0;       // march sweep z-chunks (0: the device-filling rule)
+    int dgemm = 0;        // FP64 transform tile, 32 or 64 (0: the size rule)
+    int fused = -1;       // FP64 pass as one cooperative launch: 1 yes, 0 no, -1 the size rule
+    float ms = 0;         // measured step time of the choice
+};
+static std::string tune_key(const CavityConfig& c, int precision) {
+    char k[160];
+    std::snprintf(k, sizeof k, "%d %d %d %d %.17g %.17g %d", c.nx, c.ny, c.nz, c.grid_stretch,
+                  c.grid_stretch ? c.grid_dx_wall : 0.0, c.grid_stretch ? c.grid_max_aspect : 0.0, precision);
+    return k;
+}
+static std::mutex g_tune_mutex;
+static std::map<std::string, Tuning> g_tune;
+static bool g_tune_file_read = false;
+static const char* tune_file() {
+    const char* f = std::getenv("CAVITY_TUNE_FILE");
+    return f && *f ? f : nullptr;
+}
+// the cached tuning of a key, if any (call with g_tune_mutex held)
+static const Tuning* tune_lookup(const std::string& key) {
+    if (!g_tune_file_read) {
+        g_tune_file_read = true;
+        if (const char* f = tune_file()) {
+            if (FILE* fp = std::fopen(f, "r")) {
+                char line[256];
+                while (std::fgets(line, sizeof line, fp)) {
+                    const char* bar = std::strchr(line, '|');
+                    Tuning t;
+                    if (!bar || std::sscanf(bar + 1, "%d %d %d %f", &t.chunks, &t.dgemm, &t.fused, &t.ms) != 4) continue;
+                    std::string k(line, bar - line);
+                    while (!k.empty() && k.back() == ' ') k.pop_back();
+                    g_tune[k] = t;
+                }
+                std::fclose(fp);
+            }
+        }
+    }
+    auto it = g_tune.find(key);
+    return it == g_tune.end() ? nullptr : &it->second;
+}
+static void tune_store(const std::string& key, const Tuning& t) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    tune_lookup(key);
+    g_tune[key] = t;
+    if (const char* f = tune_file()) {
+        if (FILE* fp = std::fopen(f, "a")) {
+            std::fprintf(fp, "%s | %d %d %d %.6f\n", key.c_str(), t.chunks, t.dgemm, t.fused, t.ms);
+            std::fclose(fp);
+        }
+    }
+}
+
 class SolverBase {
 public:
     virtual ~SolverBase() {}
@@ -114,6 +173,7 @@ public:
     virtual void kernel_times(double* ms) const = 0;
     virtual int kernels_per_step(int passes) const = 0;
     virtual long long pressure_passes() const = 0;
+    virtual void autotune(int steps, int* chunks, int* dgemm_tile, int* fused, float* ms) = 0;
     void step(CavityReport* r) {
         step_async(1);
         sync(r);
@@ -130,6 +190,9 @@ template <class T> class Solver : public SolverBase {
     static constexpr int kTileTZ = 4;
     static constexpr int kTileNT = sizeof(T) == 8 ? 256 : 512;     // threads: registers allow 512 in FP32
     using TileG = TileGeom<kTileTY, kTileTZ, kTileNT>;
+    // the z-march sweep (sweep_march.cuh): 32 x 8 columns of cells per CTA
+    static constexpr int kMarchTX = 32, kMarchTY = 8;
+    using MarchG = MarchGeom<kMarchTX, kMarchTY>;
 
 public:
     explicit Solver(const CavityConfig& cfg) : c_(cfg) {
@@ -160,6 +223,11 @@ public:
         allocate();
         upload_tables();
         build_graphs();
+        {
+            std::lock_guard<std::mutex> lock(g_tune_mutex);
+            if (const Tuning* t = tune_lookup(tune_key(c_, sizeof(T) == 8 ? 0 : 1))) tune_ = *t;
+        }
+        if (const char* a = std::getenv("CAVITY_AUTOTUNE")) auto_tune_ = a[0] == '1';
         check(cudaStreamSynchronize(stream_));
     }
     ~Solver() override {
@@ -194,6 +262,7 @@ public:
     }
 
     void step_async(int count) override {
+        if (auto_tune_ && tune_.ms == 0 && pending_.empty()) autotune(6, nullptr, nullptr, nullptr, nullptr);
         ensure_graphs(false);
         if (pending_.empty()) steps_before_ = hc_.steps;
         for (int i = 0; i < count; i++) {
@@ -543,6 +612,82 @@ public:
         cudaEventDestroy(e1);
     }
 
+    // Time whole steps under each candidate launch shape from the current state, restore the state after each,
+    // and keep the fastest (cached per grid size, stretching and precision; see Tuning).  Candidates: the march
+    // sweep's z-chunk count at 1/2, 1, 2 and 4 times the device-filling count, and, where the FP64 transforms
+    // run, their 32 x 32 and 64 x 64 tiles.
+    void autotune(int steps, int* chunks_out, int* dgemm_out, int* fused_out, float* ms_out) override {
+        if (!pending_.empty()) fail("autotune: steps are queued; sync first");
+        steps = std::max(steps, 2);
+        auto_tune_ = false;
+        const long long bytes = checkpoint_bytes();
+        void* saved = nullptr;
+        check(cudaMalloc(&saved, (size_t)bytes));
+        checkpoint_save(saved, 1);
+        tune_ = Tuning{};
+        const int c0 = (int)march_chunks();
+        std::vector<int> cands;
+        for (int c : {c0, c0 / 2, 2 * c0, 4 * c0}) {
+            c = std::min(std::max(c, 1), std::max(1, nz_ / 4));
+            if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
+        }
+        if (sweep_kind_ != kSweepMarch) cands = {0};
+        // FP64 transform variants: 64 x 64 tiles, 32 x 32 tiles, and 32 x 32 tiles in one cooperative launch
+        std::vector<std::pair<int, int>> tiles = {{0, -1}};
+        if (!tc_fdm_) {
+            tiles = {{64, 0}, {32, 0}};
+            if (fused_pass_capacity() > 0) tiles.push_back({32, 1});
+        }
+        cudaEvent_t e0, e1;
+        check(cudaEventCreate(&e0));
+        check(cudaEventCreate(&e1));
+        Tuning best;
+        best.ms = -1;
+        for (int c : cands)
+            for (const auto& t : tiles) {
+                Tuning cand;
+                cand.chunks = c;
+                cand.dgemm = t.first;
+                cand.fused = t.second;
+                tune_ = cand;
+                drop_graphs();
+                float ms = -1;
+                try {
+                    ensure_graphs(false);
+                    step(nullptr);                                   // warm-up (graph upload)
+                    check(cudaEventRecord(e0, stream_));
+                    for (int i = 0; i < steps; i++) {
+                        check(cudaGraphLaunch(exec_[par_], stream_));
+                        pending_.push_back(par_);
+                        par_ ^= 1;
+                    }
+                    check(cudaEventRecord(e1, stream_));
+                    sync(nullptr);
+                    check(cudaEventElapsedTime(&ms, e0, e1));
+                    ms /= steps;
+                } catch (const std::exception&) {
+                    ms = -1;                                         // a failed step: not a candidate
+                }
+                pending_.clear();
+                checkpoint_load(saved, 1);
+                if (ms > 0 && (best.ms < 0 || ms < best.ms)) {
+                    best = cand;
+                    best.ms = ms;
+                }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(saved);
+        if (best.ms < 0) best = Tuning{};
+        tune_ = best;
+        drop_graphs();
+        if (best.ms > 0) tune_store(tune_key(c_, sizeof(T) == 8 ? 0 : 1), best);
+        if (chunks_out) *chunks_out = best.chunks;
+        if (dgemm_out) *dgemm_out = best.dgemm;
+        if (fused_out) *fused_out = best.fused;
+        if (ms_out) *ms_out = best.ms;
+    }
+
     // per-step device time of the sweeps, the projection starts, the residuals of their guesses and the finishes
     // (all three stages) in the last time_steps call
     void kernel_times(double* ms) const override {
@@ -696,7 +841,10 @@ private:
         return c_.u_lid;
     }
 
-    void push_control() { check(cudaMemcpyAsync(ctrl_, &hc_, sizeof hc_, cudaMemcpyHostToDevice, stream_)); }
+    void push_control() {
+        hc_.counter[kCntBar] = 0;         // a grid barrier that timed out may have left arrivals behind
+        check(cudaMemcpyAsync(ctrl_, &hc_, sizeof hc_, cudaMemcpyHostToDevice, stream_));
+    }
     void pull_control() {
         check(cudaMemcpyAsync(&hc_, ctrl_, sizeof hc_, cudaMemcpyDeviceToHost, stream_));
         check(cudaStreamSynchronize(stream_));
@@ -709,6 +857,7 @@ private:
         case kRhsNaN: fail("pressure solve: right-hand side is NaN/inf (the run has blown up)");
         case kResidualNaN: fail("pressure solve: residual is NaN/inf");
         case kDeviceWait: fail("pressure solve: a tensor-core transform timed out waiting for its MMAs");
+        case kBarrierWait: fail("pressure solve: the one-launch FDM pass timed out at a grid barrier");
         case kNotConverged:
             std::snprintf(msg, sizeof msg, "pressure solve: residual %.2e > FDM_RTOL after %d passes", hc_.error_value,
                           hc_.error_passes);
@@ -782,10 +931,16 @@ private:
         a.r = (T)c_.reinit_r;
         a.one_minus_r = (T)(1.0 - c_.reinit_r);
         a.nu = (T)c_.nu;
-        if (tile_sweep_) {
+        if (sweep_kind_ == kSweepMarch) {
+            using G = MarchG;
+            const dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + G::TY - 1) / G::TY, march_chunks());
+            if (!record_launch(kLkSweep, kSweepMarch, grid, G::template smem_bytes<T>(), a))
+                check(launch_pdl(sweep_march_kernel<T, kMarchTX, kMarchTY>, grid, dim3(G::NT),
+                                 G::template smem_bytes<T>(), st, a));
+        } else if (sweep_kind_ == kSweepTile) {
             using G = TileG;
             dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
-            if (!record_launch(kLkSweep, 0, grid, G::template smem_bytes<T>(), a))
+            if (!record_launch(kLkSweep, kSweepTile, grid, G::template smem_bytes<T>(), a))
                 check(launch_pdl(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>, grid, dim3(kTileNT),
                                  G::template smem_bytes<T>(), st, a));
         } else {
@@ -839,7 +994,12 @@ private:
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
         if (tc_fdm_) launch_tc_pass(st, phi, h, use_h != 0);
-        else launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h != 0);
+        else {
+            const int outer = g_dgemm_tile;              // a batch's choice wins over this cavity's own tuning
+            if (!g_launch_record && tune_.dgemm) g_dgemm_tile = tune_.dgemm;
+            launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h != 0, tune_.fused);
+            g_dgemm_tile = outer;
+        }
         launch_residual(st, phi, h, use_h);
     }
     void launch_tc_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
@@ -944,13 +1104,24 @@ private:
 
     void build_graphs() {
         {
-            // momentum sweep: the shared-memory tile kernel unless CAVITY_SWEEP=face
+            // momentum sweep: shared-memory tiles unless CAVITY_SWEEP=march (the z-march, sweep_march.cuh) or =face
+            // (a thread per face).  The march evaluates each edge once but measured slower than the tiles (C2:
+            // 54.6 against 40.6 us per launch; 128^3 mixed: 196 against 133 us), so it is not the default.
             const char* sw = std::getenv("CAVITY_SWEEP");
-            tile_sweep_ = !(sw && std::string(sw) == "face");
-            using G = TileG;
-            if (tile_sweep_)
+            const std::string kind = sw ? sw : "";
+            sweep_kind_ = kind == "face" ? kSweepFace : kind == "march" ? kSweepMarch : kSweepTile;
+            if (sweep_kind_ == kSweepTile)
                 check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::template smem_bytes<T>()));
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)TileG::template smem_bytes<T>()));
+            if (sweep_kind_ == kSweepMarch) {
+                const int smem = (int)MarchG::template smem_bytes<T>();
+                check(cudaFuncSetAttribute(sweep_march_kernel<T, kMarchTX, kMarchTY>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+                check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&march_per_sm_, sweep_march_kernel<T, kMarchTX, kMarchTY>,
+                                                                    MarchG::NT, smem));
+                march_per_sm_ = std::max(1, march_per_sm_);
+            }
             if (tc_fdm_) check(tc_transform_prepare());
         }
         for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
@@ -959,6 +1130,16 @@ private:
     }
     // the step graphs of both state parities (timing: with events around the sweeps), captured on first use, so
     // a solver that only takes part in batches or is only initialised never builds them
+    void drop_graphs() {
+        for (int s = 0; s < 2; s++) {
+            if (exec_[s]) cudaGraphExecDestroy(exec_[s]);
+            if (graph_[s]) cudaGraphDestroy(graph_[s]);
+            if (texec_[s]) cudaGraphExecDestroy(texec_[s]);
+            if (tgraph_[s]) cudaGraphDestroy(tgraph_[s]);
+            exec_[s] = texec_[s] = nullptr;
+            graph_[s] = tgraph_[s] = nullptr;
+        }
+    }
     void ensure_graphs(bool timing) {
         if (eager_) return;
         for (int S = 0; S < 2; S++) {
@@ -1008,7 +1189,22 @@ private:
     cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
     int par_ = 0;
     bool eager_ = false;
-    bool tile_sweep_ = true;
+    int sweep_kind_ = kSweepTile;
+    Tuning tune_;
+    bool auto_tune_ = false;
+    int march_per_sm_ = 1;
+    // z-chunks of a march sweep launch: as many as fill the device's resident CTA slots once (all cavities of a
+    // batch together) with at least four layers per chunk; CAVITY_MARCH_CHUNKS overrides
+    unsigned int march_chunks() const {
+        const long long tiles = (long long)((nx_ + kMarchTX - 1) / kMarchTX) * ((ny_ + kMarchTY - 1) / kMarchTY) *
+                                std::max(g_launch_batch, 1);
+        long long chunks = (long long)sms_ * march_per_sm_ / tiles;
+        if (tune_.chunks > 0 && g_launch_batch <= 1) chunks = tune_.chunks;
+        if (const char* e = std::getenv("CAVITY_MARCH_CHUNKS")) chunks = std::atoll(e);
+        chunks = std::min<long long>(std::max(1LL, chunks), std::max(1, nz_ / 4));
+        const long long zc = (nz_ + chunks - 1) / chunks;
+        return (unsigned int)((nz_ + zc - 1) / zc);
+    }
     std::vector<int> pending_;
     long long steps_before_ = 0;
     // fields: three buffer sets of velocity, impulse and potential (state, stage outputs)
@@ -1071,17 +1267,26 @@ public:
     explicit Batch(const std::vector<S_*>& members) : m_(members) {
         if (m_.empty()) fail("batch: no cavities");
         const S_& f = *m_[0];
+        long long tiles64 = 0;
         for (const S_* s : m_) {
-            if (s->nx_ != f.nx_ || s->ny_ != f.ny_ || s->nz_ != f.nz_) fail("batch: every cavity needs the same grid size");
-            if (s->tc_fdm_ != f.tc_fdm_ || !s->tile_sweep_) fail("batch: every cavity needs the same kernels (tile sweep)");
+            if (s->nx_ != f.nx_ || s->ny_ != f.ny_ || s->nz_ != f.nz_) mixed_sizes_ = true;
+            tiles64 += (long long)((s->nx_ + 63) / 64) * ((s->ny_ * s->nz_ + 63) / 64);
+            if (s->tc_fdm_ != f.tc_fdm_ || s->sweep_kind_ != f.sweep_kind_ || s->sweep_kind_ == kSweepFace)
+                fail("batch: every cavity needs the same kernels (march or tile sweep)");
             if (s->eager_) fail("batch: not available with CAVITY_GRAPHS=0");
             if (!s->pending_.empty()) fail("batch: a cavity has queued steps; sync it first");
         }
+        // cavities of different sizes share one FP64 transform tile: the large one when all of them together
+        // have two 64 x 64 tiles per SM in the largest transform
+        if (mixed_sizes_) dgemm_tile_ = tiles64 >= 2 * f.sms_ ? 64 : 32;
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
         using G = TileGeom<kTY, kTZ, kNT>;
         check(cudaFuncSetAttribute(sweep_tile_batched<T, kTY, kTZ, kNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)G::template smem_bytes<T>()));
+        check(cudaFuncSetAttribute(sweep_march_batched<T, S_::kMarchTX, S_::kMarchTY>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)S_::MarchG::template smem_bytes<T>()));
         if (f.tc_fdm_) check(tc_transform_prepare_batched());
         for (int S = 0; S < 2; S++) build(S);
     }
@@ -1128,59 +1333,92 @@ public:
 
 private:
     struct RecordGuard {
-        RecordGuard(std::vector<LaunchRecord>* r, int batch) {
+        RecordGuard(std::vector<LaunchRecord>* r, int batch, int dgemm_tile) {
             g_launch_record = r;
             g_launch_batch = batch;
+            g_dgemm_tile = dgemm_tile;
         }
         ~RecordGuard() {
             g_launch_record = nullptr;
             g_launch_batch = 1;
+            g_dgemm_tile = 0;
         }
     };
+    static size_t align256(size_t n) { return (n + 255) / 256 * 256; }
     // run `fn` on every member with a recorder installed, append the argument records of each recorded launch to
     // `host` (one contiguous array per launch) and, when `launch`, issue the batched launches on `st`
     template <class F> void emit(cudaStream_t st, F fn, std::vector<unsigned char>& host, bool launch) {
         const size_t B = m_.size();
         std::vector<std::vector<LaunchRecord>> recs(B);
         for (size_t b = 0; b < B; b++) {
-            RecordGuard guard(&recs[b], (int)B);
+            RecordGuard guard(&recs[b], (int)B, dgemm_tile_);
             fn(*m_[b]);
         }
         for (size_t b = 1; b < B; b++) {
             bool same = recs[b].size() == recs[0].size();
             for (size_t j = 0; same && j < recs[0].size(); j++) {
                 const LaunchRecord &x = recs[0][j], &y = recs[b][j];
-                same = x.kind == y.kind && x.variant == y.variant && x.grid.x == y.grid.x && x.grid.y == y.grid.y &&
-                       x.grid.z == y.grid.z && x.smem == y.smem && x.args.size() == y.args.size();
+                same = x.kind == y.kind && x.variant == y.variant && x.smem == y.smem && x.args.size() == y.args.size();
             }
             if (!same) fail("batch: the cavities' launch sequences differ");
         }
+        const unsigned char* dbase = static_cast<const unsigned char*>(dargs_cur_);
         for (size_t j = 0; j < recs[0].size(); j++) {
             const size_t sz = recs[0][j].args.size();
-            const size_t off = (host.size() + 255) / 256 * 256;
+            const size_t off = align256(host.size());
             host.resize(off + sz * B);
             for (size_t b = 0; b < B; b++) std::memcpy(host.data() + off + b * sz, recs[b][j].args.data(), sz);
-            if (launch) launch_batched(recs[0][j], static_cast<const unsigned char*>(dargs_cur_) + off, (int)B, st);
+            // the work list: every cavity's blocks of its own launch grid, cavity after cavity (identical lists
+            // are stored once)
+            size_t items_off = 0, n_items = 0;
+            if (recs[0][j].kind != kLkStepBegin) {
+                std::vector<BatchItem> items;
+                for (size_t b = 0; b < B; b++) {
+                    const dim3 g = recs[b][j].grid;
+                    for (unsigned int z = 0; z < g.z; z++)
+                        for (unsigned int y = 0; y < g.y; y++)
+                            for (unsigned int x = 0; x < g.x; x++) items.push_back({(unsigned int)b, x, y, z, g.x, g.y, g.z, 0u});
+                }
+                std::string key(reinterpret_cast<const char*>(items.data()), items.size() * sizeof(BatchItem));
+                auto it = item_lists_.find(key);
+                if (it == item_lists_.end()) {
+                    items_off = align256(host.size());
+                    host.resize(items_off + key.size());
+                    std::memcpy(host.data() + items_off, key.data(), key.size());
+                    item_lists_.emplace(std::move(key), items_off);
+                } else {
+                    items_off = it->second;
+                }
+                n_items = items.size();
+            }
+            if (launch)
+                launch_batched(recs[0][j], dbase + off, reinterpret_cast<const BatchItem*>(dbase + items_off),
+                               (unsigned int)n_items, (int)B, st);
         }
     }
-    void launch_batched(const LaunchRecord& r, const void* d, int B, cudaStream_t st) {
-        const dim3 g(r.grid.x, r.grid.y, r.grid.z * B);
-        const unsigned int per = r.grid.z;
+    void launch_batched(const LaunchRecord& r, const void* d, const BatchItem* items, unsigned int n_items, int B,
+                        cudaStream_t st) {
+        const dim3 g(n_items);
         switch (r.kind) {
         case kLkStepBegin: check(launch_pdl(step_begin_batched, dim3(1, 1, B), dim3(32), 0, st, (const StepBeginArgs*)d)); break;
         case kLkSweep:
-            check(launch_pdl(sweep_tile_batched<T, kTY, kTZ, kNT>, g, dim3(kNT), r.smem, st, (const MomentumArgs<T>*)d, per));
+            if (r.variant == kSweepMarch)
+                check(launch_pdl(sweep_march_batched<T, S_::kMarchTX, S_::kMarchTY>, g, dim3(S_::MarchG::NT), r.smem, st,
+                                 (const MomentumArgs<T>*)d, items));
+            else
+                check(launch_pdl(sweep_tile_batched<T, kTY, kTZ, kNT>, g, dim3(kNT), r.smem, st,
+                                 (const MomentumArgs<T>*)d, items));
             break;
-        case kLkStart: check(launch_pdl(projection_start_batched<T>, g, dim3(kThreads), 0, st, (const StartArgs<T>*)d)); break;
-        case kLkResidual: check(launch_pdl(residual_batched, g, dim3(kThreads), 0, st, (const ResidualArgs*)d)); break;
-        case kLkFinish: check(launch_pdl(finish_batched<T>, g, dim3(kThreads), 0, st, (const FinishArgs<T>*)d)); break;
+        case kLkStart: check(launch_pdl(projection_start_batched<T>, g, dim3(kThreads), 0, st, (const StartArgs<T>*)d, items)); break;
+        case kLkResidual: check(launch_pdl(residual_batched, g, dim3(kThreads), 0, st, (const ResidualArgs*)d, items)); break;
+        case kLkFinish: check(launch_pdl(finish_batched<T>, g, dim3(kThreads), 0, st, (const FinishArgs<T>*)d, items)); break;
         case kLkDgemm64:
-            check(launch_pdl(dgemm_mma_batched<64, 64, 2, 2, 32>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, per));
+            check(launch_pdl(dgemm_mma_batched<64, 64, 2, 2, 32>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, items));
             break;
         case kLkDgemm32:
-            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 4, 64>, g, dim3(256), 0, st, (const GemmArgs<double>*)d, per));
+            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 4, 64>, g, dim3(256), 0, st, (const GemmArgs<double>*)d, items));
             break;
-        case kLkTc: launch_tc_batched(r.variant, g, per, (const TcTransformArgs*)d, st); break;
+        case kLkTc: launch_tc_batched(r.variant, g, items, (const TcTransformArgs*)d, st); break;
         default: fail("batch: unknown launch");
         }
     }
@@ -1229,10 +1467,12 @@ private:
     }
     void build(int S) {
         std::vector<unsigned char> host;
+        item_lists_.clear();
         sequence(S, host, false);
         check(cudaMalloc(&dargs_[S], std::max<size_t>(host.size(), 256)));
         dargs_cur_ = dargs_[S];
         host.clear();
+        item_lists_.clear();
         check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         sequence(S, host, true);
         check(cudaStreamEndCapture(stream_, &graph_[S]));
@@ -1246,6 +1486,9 @@ private:
     cudaGraphExec_t exec_[2] = {nullptr, nullptr};
     void* dargs_[2] = {nullptr, nullptr};
     void* dargs_cur_ = nullptr;
+    bool mixed_sizes_ = false;
+    int dgemm_tile_ = 0;
+    std::map<std::string, size_t> item_lists_;      // work lists already in the argument buffer, by content
 };
 
 static SolverBase* make_solver(const CavityConfig& c, int precision) {
@@ -1519,6 +1762,9 @@ long long cavity_estimate_bytes(const CavityConfig* config, int precision) {
 }
 int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms, float* kms) {
     return safely([&] { H(s).time_steps(warmup, steps, flush_l2, ms, kms); });
+}
+int cavity_autotune(CavitySolver* s, int steps, int* march_chunks, int* dgemm_tile, int* fused_pass, float* ms_per_step) {
+    return safely([&] { H(s).autotune(steps, march_chunks, dgemm_tile, fused_pass, ms_per_step); });
 }
 int cavity_kernel_times(CavitySolver* s, double* ms) {
     return safely([&] { H(s).kernel_times(ms); });

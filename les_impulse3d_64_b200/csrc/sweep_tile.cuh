@@ -378,12 +378,12 @@ template <class T, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) sweep_tile_kernel(MomentumArgs<T> a) {
     sweep_tile_body<T, TY, TZ, NT>(a, real_blk());
 }
-// a batch of cavities: grid z runs over cavities x `per` z-tiles
+// a batch of cavities: grid x runs over the work list (BatchItem)
 template <class T, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) sweep_tile_batched(const MomentumArgs<T>* args, unsigned int per) {
+__global__ void __launch_bounds__(NT) sweep_tile_batched(const MomentumArgs<T>* args, const BatchItem* items) {
     __shared__ MomentumArgs<T> a;
     int cav;
-    const Blk k = batch_blk(per, cav);
+    const Blk k = item_blk(items, cav);
     load_args(a, args + cav);
     sweep_tile_body<T, TY, TZ, NT>(a, k);
 }

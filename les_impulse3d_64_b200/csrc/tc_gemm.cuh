@@ -436,12 +436,12 @@ template <int BN, int FA, int F64>
 __global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArgs g) {
     tc_transform_body<BN, FA, F64>(g, real_blk(), first_block());
 }
-// a batch of cavities: grid z runs over cavities x `per` transform batches
+// a batch of cavities: grid x runs over the work list (BatchItem)
 template <int BN, int FA, int F64>
-__global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTransformArgs* args, unsigned int per) {
+__global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTransformArgs* args, const BatchItem* items) {
     __shared__ TcTransformArgs g;
     int cav;
-    const Blk k = batch_blk(per, cav);
+    const Blk k = item_blk(items, cav);
     load_args(g, args + cav);
     tc_transform_body<BN, FA, F64>(g, k, first_block());
 }
@@ -482,17 +482,18 @@ inline cudaError_t tc_transform_prepare_batched() {
     return e;
 }
 template <int BN>
-inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
+inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, const BatchItem* items, const TcTransformArgs* d,
+                                 cudaStream_t st) {
     const dim3 block(kTcThreads);
-    if (fa && f64) launch_pdl(tc_transform_batched<BN, 1, 1>, grid, block, TcSmem<BN>::kBytes, st, d, per);
-    else if (fa) launch_pdl(tc_transform_batched<BN, 1, 0>, grid, block, TcSmem<BN>::kBytes, st, d, per);
-    else launch_pdl(tc_transform_batched<BN, 0, 0>, grid, block, TcSmem<BN>::kBytes, st, d, per);
+    if (fa && f64) launch_pdl(tc_transform_batched<BN, 1, 1>, grid, block, TcSmem<BN>::kBytes, st, d, items);
+    else if (fa) launch_pdl(tc_transform_batched<BN, 1, 0>, grid, block, TcSmem<BN>::kBytes, st, d, items);
+    else launch_pdl(tc_transform_batched<BN, 0, 0>, grid, block, TcSmem<BN>::kBytes, st, d, items);
 }
 // a recorded launch (variant: see tc_variant) over a batch of cavities
-inline void launch_tc_batched(int variant, dim3 grid, unsigned int per, const TcTransformArgs* d, cudaStream_t st) {
+inline void launch_tc_batched(int variant, dim3 grid, const BatchItem* items, const TcTransformArgs* d, cudaStream_t st) {
     const int bn = variant & 0xff, fa = (variant >> 8) & 1, f64 = (variant >> 9) & 1;
-    if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, per, d, st);
-    else launch_tc_batched_bn<32>(fa, f64, grid, per, d, st);
+    if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, items, d, st);
+    else launch_tc_batched_bn<32>(fa, f64, grid, items, d, st);
 }
 inline cudaError_t tc_transform_prepare() {
     cudaError_t e = tc_prepare_bn<64>();

@@ -2,10 +2,12 @@
 
 Two ways of stepping them:
 
-* batched (the default): cavities of the same grid size and precision form are grouped into batches
-  (`cavity_batch_create`).  One CUDA graph steps a whole batch, and each of its kernel launches covers every
-  cavity of the batch, so a step of B cavities costs the launches of one.  Batches of different sizes run on
-  their own streams, concurrently.
+* batched (the default): cavities of the same precision form are grouped into batches (`cavity_batch_create`),
+  whatever their grid sizes.  One CUDA graph steps a whole batch, and each of its kernel launches covers every
+  cavity of the batch through a work list of (cavity, block) entries, so a step of B cavities costs the launches
+  of one.  Cavities whose launch sequences differ (the tensor-core transforms of the mixed form from 128^3 cells
+  up, for instance) go to separate batches, by size, which run on their own streams, concurrently.
+  `group='size'` batches by grid size only.
 * per cavity (`batched=False`): every cavity steps through its own stream and graphs; the graph launches of all
   cavities are enqueued before waiting for any, so small, latency-bound kernels of different cavities overlap.
 
@@ -19,8 +21,9 @@ from .api import Batch, Cavity
 
 
 class Ensemble:
-    def __init__(self, cases, library=None, batched=True):
-        """`cases`: dicts with `settings`, `noise`, `seed` and `precision` (see workloads.ensemble_cases)."""
+    def __init__(self, cases, library=None, batched=True, group='precision'):
+        """`cases`: dicts with `settings`, `noise`, `seed` and `precision` (see workloads.ensemble_cases);
+        `group`: 'precision' (one batch per precision form where the launch sequences agree) or 'size'."""
         self.cases = list(cases)
         self.cavities = []
         self.batches = []
@@ -31,16 +34,38 @@ class Ensemble:
                 self.cavities.append(cav)
                 cav.initialize(*workloads.initial_noise(cav.shapes, case['noise'], case['seed']))
             if batched:
-                keys = {}
+                by_size, by_form = {}, {}
                 for i, (case, cav) in enumerate(zip(self.cases, self.cavities)):
-                    keys.setdefault((cav.nx, cav.ny, cav.nz, case.get('precision', 'mixed')), []).append(i)
-                for members in keys.values():
+                    form = case.get('precision', 'mixed')
+                    by_size.setdefault((cav.nx, cav.ny, cav.nz, form), []).append(i)
+                    by_form.setdefault(form, []).append(i)
+                groups = list(by_size.values())
+                if group == 'precision':
+                    groups = []
+                    for form, members in by_form.items():
+                        sizes = [k for k in by_size if k[3] == form]
+                        if len(sizes) > 1 and self._try_batch(members):
+                            continue
+                        groups += [by_size[k] for k in sizes]
+                for members in groups:
                     self.batches.append(Batch([self.cavities[i] for i in members]))
                     self.groups.append(members)
         except Exception:
             self.close()
             raise
         self.cells = [c.n_cell for c in self.cavities]
+
+    def _try_batch(self, members):
+        """One batch of cavities of different sizes; False when their launch sequences differ."""
+        try:
+            batch = Batch([self.cavities[i] for i in members])
+        except RuntimeError as exc:
+            if 'launch sequences differ' in str(exc):
+                return False
+            raise
+        self.batches.append(batch)
+        self.groups.append(members)
+        return True
 
     def advance(self, steps, chunk=8):
         """Advance every cavity by `steps` steps, `chunk` queued per cavity (or batch) between waits; returns the

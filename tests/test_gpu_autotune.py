@@ -1,0 +1,41 @@
+"""The autotuner (cavity_autotune): it leaves the cavity's state as it was, picks one of its candidates, and the
+steps it then runs are bit-identical to an untuned cavity's; the choice is written to CAVITY_TUNE_FILE."""
+import numpy as np
+import pytest
+
+from les_impulse3d_64_b200 import workloads
+from les_impulse3d_64_b200.api import Cavity
+
+pytestmark = pytest.mark.gpu
+FIELDS = ('u', 'v', 'w', 'mx', 'my', 'mz', 'phi')
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
+def test_autotune_keeps_state_and_results(precision, tmp_path, monkeypatch):
+    tune_file = tmp_path / 'tune.txt'
+    monkeypatch.setenv('CAVITY_TUNE_FILE', str(tune_file))
+    s = workloads.settings(48, 1000.0, nz=40, beta=1.5, cfl=0.5)
+    a, b = Cavity(s, precision=precision), Cavity(s, precision=precision)
+    try:
+        for cav in (a, b):
+            cav.initialize(*workloads.initial_noise(cav.shapes, 1e-3, 4))
+            for _ in range(3):
+                cav.step()
+        before = {k: a.field(k) for k in FIELDS}
+        rep = a.report()
+        chunks, tile, fused, ms = a.autotune(steps=3)
+        # FP64 transforms below 128^3 in both forms: 64 x 64 or 32 x 32 tiles, the latter possibly in one launch
+        assert ms > 0 and 1 <= chunks <= 40 // 4 and (tile, fused) in ((64, 0), (32, 0), (32, 1))
+        assert a.report() == rep
+        for k in FIELDS:
+            assert np.array_equal(a.field(k), before[k]), k
+        for _ in range(4):
+            ra, rb = a.step(), b.step()
+            assert ra == rb
+        for k in FIELDS:
+            assert np.array_equal(a.field(k), b.field(k)), k
+    finally:
+        a.close()
+        b.close()
+    line = tune_file.read_text().strip().splitlines()[-1]
+    assert line.startswith('48 48 40 1 ') and line.split('|')[1].split()[:3] == [str(chunks), str(tile), str(fused)]

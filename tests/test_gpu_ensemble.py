@@ -10,8 +10,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize('batched', [True, False])
 def test_ensemble_matches_alone(batched):
-    """Batched (one graph per group of same-size cavities) or per-cavity stepping: bit-identical to each cavity
-    stepped alone."""
+    """Batched (one graph for the cavities of each precision form, whatever their sizes) or per-cavity stepping:
+    bit-identical to each cavity stepped alone."""
     cases = workloads.ensemble_cases(count=9, seed=3, sizes=(12, 16, 24), re_range=(100.0, 2000.0))
     for k, c in enumerate(cases):          # batches mixing uniform and stretched grids, in both forms
         c['precision'] = 'mixed' if k < 5 else 'fp64'
@@ -45,3 +45,29 @@ def test_many_mixed_cavities_set_up_and_converge():
             assert rep['steps'] == 2 and rep['phi_rel'] <= 1e-9
     finally:
         ens.close()
+
+
+@pytest.mark.parametrize('group', ['precision', 'size'])
+def test_large_mixed_size_batch_matches_alone(group):
+    """48 cavities of three sizes in one batch: enough transform tiles that the batch runs the large FP64
+    transform tile, and few z-chunks per cavity in the column kernels, where a cavity alone fills the device with
+    its own.  Its reductions (norms, the mean of the potential) then add the same values in another grouping, so
+    each cavity ends equal to itself alone to rounding: 1e-6 relative in the FP32 fields of the mixed form."""
+    cases = workloads.ensemble_cases(count=48, seed=7, sizes=(16, 24, 32), re_range=(100.0, 2000.0))
+    ens = Ensemble(cases, group=group)
+    try:
+        assert len(ens.batches) == (1 if group == 'precision' else 3)
+        ens.advance(4, chunk=2)
+        together = [ens.fields(i) for i in range(len(cases))]
+    finally:
+        ens.close()
+    for i in (0, 17, 47):
+        alone = Ensemble([cases[i]], batched=False)
+        try:
+            alone.advance(4, chunk=1)
+            f = alone.fields(0)
+        finally:
+            alone.close()
+        for k in f:
+            err = float(np.abs(f[k] - together[i][k]).max() / max(np.abs(f[k]).max(), 1e-30))
+            assert err <= 1e-6, (i, k, err)

@@ -51,14 +51,20 @@ def call_fdm(lib, name, S, inv_lambda, r, phi):
     return dphi.cpu().numpy()
 
 
-@pytest.mark.parametrize('dims', [(8, 8, 5), (24, 24, 16), (40, 40, 33)])
-def test_fdm_pass_matches_numpy(dims):
+@pytest.mark.parametrize('fused', ['0', '1'])
+@pytest.mark.parametrize('dims', [(8, 8, 5), (24, 24, 16), (40, 40, 33), (64, 64, 64), (96, 80, 70)])
+def test_fdm_pass_matches_numpy(dims, fused, monkeypatch):
+    """The FP64 pass as six launches (CAVITY_FDM_FUSED=0) and as one cooperative launch with grid barriers
+    between the transforms (=1), each against NumPy; and the two bit for bit against each other."""
+    monkeypatch.setenv('CAVITY_FDM_FUSED', fused)
     lib = load_library()
     lib.cavity_last_error.restype = ct.c_char_p
     S, il, r, phi = random_operands(*dims, seed=sum(dims))
     out = call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi)
     ref = fdm_reference(S, r, il, phi)
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+    monkeypatch.setenv('CAVITY_FDM_FUSED', '1' if fused == '0' else '0')
+    assert np.array_equal(call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi), out)
 
 
 @pytest.mark.parametrize('dims', [(8, 8, 5), (24, 24, 16), (40, 40, 33), (64, 64, 64), (128, 96, 130)])
