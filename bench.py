@@ -42,6 +42,9 @@ def parse_args():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-batched', action='store_true',
                     help='skip the batched mixed-form sub-measurements of the default line')
+    ap.add_argument('--no-serving', action='store_true', help='skip the served-stream sub-measurement of the default line')
+    ap.add_argument('--serving-requests', type=int, default=200, help='requests of the default line\'s served stream')
+    ap.add_argument('--serving-t-end', type=float, default=0.2, help='end time of each request of that stream')
     ap.add_argument('--count', type=int, default=256, help='cavities of the c4_ensemble workload')
     ap.add_argument('--chunk', type=int, default=8, help='steps queued per cavity between waits (ensemble)')
     ap.add_argument('--requests', type=int, default=64, help='requests of the c5_serving stream')
@@ -265,6 +268,21 @@ def batched_rates(steps, warmup, chunk=8):
     return out
 
 
+def serving_sample(requests, rate, t_end, chunk=8):
+    """The C5 stream (sizes 32^3 .. 128^3, Re log-uniform in [100, 5000], half uniform and half regularised
+    lids, Poisson arrivals at `rate`), `requests` requests to `t_end`, served in real time twice: by the mixed
+    form in slot batches, and by the plain FP64 form one request at a time through its own graphs."""
+    from les_impulse3d_64_b200.serve import Server, serving_requests, summary
+    reqs = serving_requests(requests, rate, seed=0, t_end=t_end, with_fields=True)
+    ours = summary(Server(budget_bytes=120e9, precision='mixed', chunk=chunk).run(reqs))
+    plain = summary(Server(budget_bytes=120e9, precision='fp64', chunk=chunk, batched=False, max_running=1).run(reqs))
+    return {'requests': requests, 'rate_per_s': rate, 't_end': t_end, 'chunk': chunk,
+            'sizes': '32^3, 64^3, 64x64x128, 96^3, 128^3', 'budget_bytes': 120e9,
+            'served_mixed_slot_batches': ours, 'plain_fp64_one_at_a_time': plain,
+            'p50_ratio': plain['p50_s'] / ours['p50_s'], 'p99_ratio': plain['p99_s'] / ours['p99_s'],
+            'throughput_ratio': ours['cell_updates_per_s'] / plain['cell_updates_per_s']}
+
+
 def run_ours(args, ranks):
     from les_impulse3d_64_b200 import _build, workloads
     from les_impulse3d_64_b200.api import Cavity, Solver
@@ -362,6 +380,8 @@ def run_ours(args, ranks):
             v['value'] = ranks.world * v['value'] * (v['seconds'] / ranks.max(v['seconds']))
             v['ratio_vs_value'] = v['value'] / value
         line['batched'] = sub
+    if not args.no_serving and args.workload == 'c2_64cube_re1000' and ranks.world == 1:
+        line['serving'] = serving_sample(args.serving_requests, 50.0, args.serving_t_end)
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
         rate, n, dt = cpu_oracle_rate(args.workload)
         line['cpu_baseline'] = {'value': rate, 'unit': 'cell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
@@ -422,6 +442,8 @@ def run_serving(args, ranks):
         ours = summary(Server(budget_bytes=120e9, precision=args.precision or 'mixed', chunk=args.chunk).run(reqs))
     plain = summary(Server(budget_bytes=120e9, precision='fp64', chunk=args.chunk, batched=False,
                            max_running=1).run(reqs))
+    ours['p50_ratio_vs_plain'] = plain['p50_s'] / ours['p50_s']
+    ours['throughput_ratio_vs_plain'] = ours['cell_updates_per_s'] / plain['cell_updates_per_s']
     p99 = ranks.max(ours['p99_s'])
     return {
         'metric': 'p99 time-to-solution', 'value': p99, 'unit': 's', 'n_gpus': ranks.world, 'steps': None,

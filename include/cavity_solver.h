@@ -143,15 +143,26 @@ int cavity_sync_outputs(CavitySolver* s, CavityReport* r, float* probes, int max
 long long cavity_checkpoint_bytes(const CavitySolver* s);
 int cavity_checkpoint_save(CavitySolver* s, void* dst, int dst_is_device);
 int cavity_checkpoint_load(CavitySolver* s, const void* src, int src_is_device);
-/* Batches (no counterpart in the reference): cavities of the same grid size and precision form stepped
- * together by one CUDA graph per step, each of whose kernel launches covers every cavity.  Every cavity keeps
- * its own dt, pass count, clock and errors, and stays usable through its own handle between steps.  The
- * members must have no queued steps when the batch is created; destroy the batch before its members.
- * cavity_batch_sync waits for the queued steps and fills `reports` (one per member, in order); if a member's
- * step failed it reports that member's last good state and returns 1 with the error, naming the member.  A
- * batch whose members' states have diverged (a failed step) refuses further steps. */
+/* Batches (no counterpart in the reference): cavities of one precision form stepped together by one CUDA graph
+ * per step, each of whose kernel launches covers every cavity through a work list of (cavity, block) entries,
+ * so the cavities may differ in grid size.  Every cavity keeps its own dt, pass count, clock and errors, and
+ * stays usable through its own handle between steps.  The members must have no queued steps when the batch is
+ * created; take a cavity out of the batch (or destroy the batch) before destroying the cavity.
+ * cavity_batch_sync waits for the queued steps and fills `reports` (one per slot, in order; an empty slot's
+ * report is zero with steps = -1); if a member's step failed it reports that member's last good state and
+ * returns 1 with the error, naming the slot.  A batch whose members' states have diverged (a failed step)
+ * refuses further steps.
+ * cavity_batch_create_slots makes a batch of `capacity` slots, the first `count` holding `members`, the rest
+ * empty (the members then need one grid size).  cavity_batch_set_member puts a cavity of the batch's grid
+ * size, form and kernels into a slot, or empties it (s = NULL), without rebuilding the batch's graphs: it
+ * rewrites the slot's argument records and live flag in the device buffers the graphs read, so a served stream
+ * of requests joins and leaves a running batch.  It needs no queued steps, and the cavity may be at either
+ * state parity.  Blocks of an empty slot return at once. */
 typedef struct CavityBatch CavityBatch;
 int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** out);
+int cavity_batch_create_slots(CavitySolver* const* members, int count, int capacity, CavityBatch** out);
+int cavity_batch_set_member(CavityBatch* b, int slot, CavitySolver* s);
+int cavity_batch_size(const CavityBatch* b);
 int cavity_batch_step_async(CavityBatch* b, int count);
 int cavity_batch_sync(CavityBatch* b, CavityReport* reports);
 int cavity_batch_destroy(CavityBatch* b);

@@ -385,22 +385,39 @@ class Cavity:
 
 
 class Batch:
-    """Cavities of the same grid size and form stepped together (cavity_batch_* functions): every kernel launch
-    of a batched step covers all of them.  The cavities stay ordinary `Cavity` handles between steps (fields,
-    probes, diagnostics); close the batch before closing them."""
+    """Cavities of one precision form stepped together (cavity_batch_* functions): every kernel launch of a
+    batched step covers all of them, whatever their grid sizes.  With `capacity` above the number of cavities
+    the batch has empty slots (its cavities then need one grid size); `set_member` puts a cavity into a slot or
+    empties it without rebuilding the batch's graphs.  The cavities stay ordinary `Cavity` handles between steps
+    (fields, probes, diagnostics); take a cavity out of the batch, or close the batch, before closing it."""
 
-    def __init__(self, cavities):
+    def __init__(self, cavities, capacity=None):
         if not cavities:
             raise ValueError('a batch needs at least one cavity')
-        self.cavities = list(cavities)
-        self.lib = L = self.cavities[0].lib
-        L.cavity_batch_create.argtypes = [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_void_p)]
+        cavities = list(cavities)
+        capacity = len(cavities) if capacity is None else max(int(capacity), len(cavities))
+        self.slots = cavities + [None] * (capacity - len(cavities))
+        self.lib = L = cavities[0].lib
+        L.cavity_batch_create_slots.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ct.c_void_p)]
+        L.cavity_batch_set_member.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p]
         L.cavity_batch_step_async.argtypes = [ct.c_void_p, ct.c_int]
         L.cavity_batch_sync.argtypes = [ct.c_void_p, ct.c_void_p]
         L.cavity_batch_destroy.argtypes = [ct.c_void_p]
-        handles = (ct.c_void_p * len(self.cavities))(*[c.handle.value for c in self.cavities])
+        handles = (ct.c_void_p * len(cavities))(*[c.handle.value for c in cavities])
         self.handle = ct.c_void_p()
-        self._call('cavity_batch_create', handles, len(self.cavities), ct.byref(self.handle))
+        self._call('cavity_batch_create_slots', handles, len(cavities), capacity, ct.byref(self.handle))
+
+    @property
+    def cavities(self):
+        return [c for c in self.slots if c is not None]
+
+    def free_slots(self):
+        return [i for i, c in enumerate(self.slots) if c is None]
+
+    def set_member(self, slot, cavity):
+        """Put `cavity` into slot `slot`, or empty the slot (None); no steps may be queued."""
+        self._call('cavity_batch_set_member', self.handle, int(slot), None if cavity is None else cavity.handle)
+        self.slots[slot] = cavity
 
     def _call(self, name, *args):
         if getattr(self.lib, name)(*args):
@@ -410,10 +427,10 @@ class Batch:
         self._call('cavity_batch_step_async', self.handle, int(count))
 
     def sync(self):
-        """Wait for the queued steps; the report of every cavity."""
-        reports = (Report * len(self.cavities))()
+        """Wait for the queued steps; the report of every slot (None for an empty slot)."""
+        reports = (Report * len(self.slots))()
         self._call('cavity_batch_sync', self.handle, reports)
-        return [Solver._as_dict(r) for r in reports]
+        return [Solver._as_dict(r) if c is not None else None for r, c in zip(reports, self.slots)]
 
     def close(self):
         if self.handle:

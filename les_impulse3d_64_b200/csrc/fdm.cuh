@@ -143,10 +143,11 @@ __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_kernel(GemmA
 // a batch of cavities: grid x runs over the work list (BatchItem)
 template <int BM, int BN, int WARPS_M, int WARPS_N, int KC>
 __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_batched(const GemmArgs<double>* args,
-                                                                            const BatchItem* items) {
+                                                                            const BatchItem* items, const int* live) {
     __shared__ GemmArgs<double> g;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(g, args + cav);
     dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, k, first_block());
 }

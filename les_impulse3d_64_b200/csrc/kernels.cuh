@@ -197,9 +197,10 @@ __device__ __forceinline__ Blk real_blk() { return {blockIdx.x, blockIdx.y, bloc
 struct BatchItem {
     unsigned int cav, x, y, z, nx, ny, nz, pad;
 };
-__device__ __forceinline__ Blk item_blk(const BatchItem* items, int& cavity) {
+// `live` holds one flag per slot of the batch: the blocks of an empty slot return at once (see Batch::set_member)
+__device__ __forceinline__ Blk item_blk(const BatchItem* items, const int* live, int& cavity) {
     const BatchItem it = items[blockIdx.x];
-    cavity = (int)it.cav;
+    cavity = live[it.cav] ? (int)it.cav : -1;
     return {it.x, it.y, it.z, it.nx, it.ny, it.nz};
 }
 __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0; }
@@ -324,7 +325,8 @@ __global__ void step_begin_kernel(Params p, Control* c) {
     if (blockIdx.x == 0) step_begin_body(p, c);
 }
 // one block per cavity of the batch
-__global__ void step_begin_batched(const StepBeginArgs* args) {
+__global__ void step_begin_batched(const StepBeginArgs* args, const int* live) {
+    if (!live[blockIdx.z]) return;
     const StepBeginArgs& a = args[blockIdx.z];
     step_begin_body(a.p, a.c);
 }
@@ -549,10 +551,11 @@ __global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_kern
     projection_start_body(a, real_blk());
 }
 template <class T>
-__global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_batched(const StartArgs<T>* args, const BatchItem* items) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) projection_start_batched(const StartArgs<T>* args, const BatchItem* items, const int* live) {
     __shared__ StartArgs<T> a;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(a, args + cav);
     projection_start_body(a, k);
 }
@@ -688,10 +691,11 @@ __device__ void residual_body(const ResidualArgs& a, const Blk& k) {
     }
 }
 __global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_kernel(ResidualArgs a) { residual_body(a, real_blk()); }
-__global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_batched(const ResidualArgs* args, const BatchItem* items) {
+__global__ void __launch_bounds__(kThreads, kResidualBlocks) residual_batched(const ResidualArgs* args, const BatchItem* items, const int* live) {
     __shared__ ResidualArgs a;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(a, args + cav);
     residual_body(a, k);
 }
@@ -871,10 +875,11 @@ __device__ void finish_body(const FinishArgs<T>& a, const Blk& k) {
 template <class T>
 __global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_kernel(FinishArgs<T> a) { finish_body(a, real_blk()); }
 template <class T>
-__global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_batched(const FinishArgs<T>* args, const BatchItem* items) {
+__global__ void __launch_bounds__(kThreads, kColumnBlocks) finish_batched(const FinishArgs<T>* args, const BatchItem* items, const int* live) {
     __shared__ FinishArgs<T> a;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(a, args + cav);
     finish_body(a, k);
 }

@@ -1257,6 +1257,7 @@ public:
     virtual void step_async(int count) = 0;
     virtual void sync(CavityReport* reports) = 0;
     virtual int size() const = 0;
+    virtual void set_member(int slot, SolverBase* s) = 0;
 };
 
 template <class T> class Batch : public BatchBase {
@@ -1264,21 +1265,35 @@ template <class T> class Batch : public BatchBase {
     static constexpr int kTY = S_::kTileTY, kTZ = S_::kTileTZ, kNT = S_::kTileNT;
 
 public:
-    explicit Batch(const std::vector<S_*>& members) : m_(members) {
+    // `members` fill slots 0 .. n-1 of `capacity` slots; the other slots start empty (cavities of one size only)
+    Batch(const std::vector<S_*>& members, int capacity) : m_(members) {
         if (m_.empty()) fail("batch: no cavities");
         const S_& f = *m_[0];
         long long tiles64 = 0;
         for (const S_* s : m_) {
             if (s->nx_ != f.nx_ || s->ny_ != f.ny_ || s->nz_ != f.nz_) mixed_sizes_ = true;
             tiles64 += (long long)((s->nx_ + 63) / 64) * ((s->ny_ * s->nz_ + 63) / 64);
-            if (s->tc_fdm_ != f.tc_fdm_ || s->sweep_kind_ != f.sweep_kind_ || s->sweep_kind_ == kSweepFace)
-                fail("batch: every cavity needs the same kernels (march or tile sweep)");
-            if (s->eager_) fail("batch: not available with CAVITY_GRAPHS=0");
-            if (!s->pending_.empty()) fail("batch: a cavity has queued steps; sync it first");
+            check_member(s, f);
         }
+        for (size_t i = 0; i < m_.size(); i++)
+            for (size_t k = 0; k < i; k++)
+                if (m_[i] == m_[k]) fail("batch: a cavity appears twice");
+        if (capacity < (int)m_.size()) capacity = (int)m_.size();
+        if (capacity > (int)m_.size() && mixed_sizes_) fail("batch: empty slots need cavities of one grid size");
         // cavities of different sizes share one FP64 transform tile: the large one when all of them together
         // have two 64 x 64 tiles per SM in the largest transform
         if (mixed_sizes_) dgemm_tile_ = tiles64 >= 2 * f.sms_ ? 64 : 32;
+        proto_ = m_[0];
+        par_ = m_[0]->par_;
+        nx_ = f.nx_;
+        ny_ = f.ny_;
+        nz_ = f.nz_;
+        tc_fdm_ = f.tc_fdm_;
+        sweep_kind_ = f.sweep_kind_;
+        m_.resize(capacity, nullptr);
+        d_.assign(capacity, 0);
+        for (int i = 0; i < capacity; i++)
+            if (m_[i]) d_[i] = m_[i]->par_ ^ par_;
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
         using G = TileGeom<kTY, kTZ, kNT>;
@@ -1289,6 +1304,7 @@ public:
                                    (int)S_::MarchG::template smem_bytes<T>()));
         if (f.tc_fdm_) check(tc_transform_prepare_batched());
         for (int S = 0; S < 2; S++) build(S);
+        proto_ = nullptr;        // members may leave and be destroyed from now on
     }
     ~Batch() override {
         if (stream_) cudaStreamSynchronize(stream_);
@@ -1304,23 +1320,34 @@ public:
 
     void step_async(int count) override {
         for (int i = 0; i < count; i++) {
-            const int S = m_[0]->par_;
-            for (const S_* s : m_)
-                if (s->par_ != S) fail("batch: the cavities' states have diverged (a failed step); rebuild the batch");
-            check(cudaGraphLaunch(exec_[S], stream_));
+            for (size_t k = 0; k < m_.size(); k++)
+                if (m_[k] && m_[k]->par_ != (par_ ^ d_[k]))
+                    fail("batch: the cavities' states have diverged (a failed step); rebuild the batch");
+            check(cudaGraphLaunch(exec_[par_], stream_));
             for (S_* s : m_) {
+                if (!s) continue;
                 if (s->pending_.empty()) s->steps_before_ = s->hc_.steps;
                 s->pending_.push_back(s->par_);
                 s->par_ ^= 1;
             }
+            par_ ^= 1;
+            queued_ = true;
         }
     }
-    // waits for the queued steps; every cavity's report (its last good state if it failed), then the first
-    // failure as an error naming the cavity
+    // waits for the queued steps; every occupied slot's report (its last good state if it failed; an empty
+    // slot's report is zero with steps = -1), then the first failure as an error naming the slot
     void sync(CavityReport* reports) override {
         check(cudaStreamSynchronize(stream_));
+        queued_ = false;
         std::string first;
         for (size_t i = 0; i < m_.size(); i++) {
+            if (!m_[i]) {
+                if (reports) {
+                    std::memset(&reports[i], 0, sizeof(CavityReport));
+                    reports[i].steps = -1;
+                }
+                continue;
+            }
             try {
                 m_[i]->sync(reports ? &reports[i] : nullptr);
             } catch (const std::exception& e) {
@@ -1329,6 +1356,47 @@ public:
             }
         }
         if (!first.empty()) fail(first);
+    }
+    // Put cavity `s` into slot `slot` (nullptr: empty the slot) without rebuilding the step graphs: its
+    // argument records for both graphs and the slot's live flag are written into the device buffers the graphs
+    // read.  A newly placed cavity need not be at the batch's state parity (the slot keeps the offset).
+    void set_member(int slot, SolverBase* base) override {
+        if (slot < 0 || slot >= (int)m_.size()) fail("batch: slot out of range");
+        if (queued_) fail("batch: steps are queued; sync first");
+        S_* s = nullptr;
+        if (base) {
+            s = dynamic_cast<S_*>(base);
+            if (!s) fail("batch: the cavity's precision form differs from the batch's");
+            for (size_t k = 0; k < m_.size(); k++)
+                if (m_[k] == s && (int)k != slot) fail("batch: the cavity is already in another slot");
+            check_member(s, *s);
+            if (s->nx_ != nx_ || s->ny_ != ny_ || s->nz_ != nz_) fail("batch: the cavity's grid size differs from the batch's");
+            if (s->tc_fdm_ != tc_fdm_ || s->sweep_kind_ != sweep_kind_) fail("batch: the cavity's kernels differ from the batch's");
+            d_[slot] = s->par_ ^ par_;
+            for (int S = 0; S < 2; S++) {
+                std::vector<LaunchRecord> rec;
+                {
+                    RecordGuard guard(&rec, (int)m_.size(), dgemm_tile_);
+                    record_member(*s, S ^ d_[slot], S);
+                }
+                const Layout& L = layout_[S];
+                if (rec.size() != L.launches.size()) fail("batch: the cavity's launch sequence differs from the batch's");
+                for (size_t j = 0; j < rec.size(); j++) {
+                    const LaunchSlot& ls = L.launches[j];
+                    if (rec[j].kind != ls.kind || rec[j].variant != ls.variant || rec[j].smem != ls.smem ||
+                        rec[j].args.size() != ls.size || rec[j].grid.x != ls.grid.x || rec[j].grid.y != ls.grid.y ||
+                        rec[j].grid.z != ls.grid.z)
+                        fail("batch: the cavity's launch sequence differs from the batch's");
+                    std::memcpy(host_[S].data() + ls.off + (size_t)slot * ls.size, rec[j].args.data(), ls.size);
+                }
+            }
+        }
+        m_[slot] = s;
+        for (int S = 0; S < 2; S++) {
+            reinterpret_cast<int*>(host_[S].data() + layout_[S].live)[slot] = s ? 1 : 0;
+            check(cudaMemcpyAsync(dargs_[S], host_[S].data(), host_[S].size(), cudaMemcpyHostToDevice, stream_));
+        }
+        check(cudaStreamSynchronize(stream_));
     }
 
 private:
@@ -1345,14 +1413,58 @@ private:
         }
     };
     static size_t align256(size_t n) { return (n + 255) / 256 * 256; }
-    // run `fn` on every member with a recorder installed, append the argument records of each recorded launch to
-    // `host` (one contiguous array per launch) and, when `launch`, issue the batched launches on `st`
-    template <class F> void emit(cudaStream_t st, F fn, std::vector<unsigned char>& host, bool launch) {
+    static void check_member(const S_* s, const S_& f) {
+        if (s->tc_fdm_ != f.tc_fdm_ || s->sweep_kind_ != f.sweep_kind_ || s->sweep_kind_ == kSweepFace)
+            fail("batch: every cavity needs the same kernels (march or tile sweep)");
+        if (s->eager_) fail("batch: not available with CAVITY_GRAPHS=0");
+        if (!s->pending_.empty()) fail("batch: a cavity has queued steps; sync it first");
+    }
+
+    // where one recorded launch's argument records sit in the argument buffer of a graph
+    struct LaunchSlot {
+        int kind, variant;
+        size_t smem, off, size;
+        dim3 grid;
+    };
+    struct Layout {
+        std::vector<LaunchSlot> launches;
+        size_t live = 0;                       // the slots' live flags (int each)
+    };
+
+    // The launches of one cavity's step, for the cavity's state parity Sm inside the graph of batch parity S
+    // (whose while-node handles the loop kernels set), in the order the graph runs them.  `part` selects one
+    // piece of the sequence (see sequence); -1 all of them.
+    void member_part(S_& s, int Sm, int S, int stage, int part) {
+        const int Xs = Sm ^ 1, Ys = 2;
+        const int in = stage == 0 ? Sm : stage == 1 ? Xs : Ys;
+        const int out = stage == 1 ? Ys : Xs;
+        const int cur = stage == 1 ? Xs : Ys;
+        const cudaGraphConditionalHandle h = handles_[S][stage];
+        cudaStream_t st = part == 3 ? body_stream_ : stream_;
+        switch (part) {
+        case 0: s.launch_momentum(st, stage, Sm, in, out); break;
+        case 1: s.launch_start(st, s.M_[out], true, stage, Sm, cur, h, 2); break;
+        case 2:
+        case 3: s.launch_pass(st, s.praw_, h, 2); break;
+        case 4: s.launch_finish(st, s.M_[out], s.U_[out], s.PHI_[out], true, stage, stage == 2); break;
+        }
+    }
+    void record_member(S_& s, int Sm, int S) {
+        s.launch_step_begin(stream_);
+        for (int stage = 0; stage < 3; stage++)
+            for (int part = 0; part < 5; part++) member_part(s, Sm, S, stage, part);
+    }
+
+    // run `fn(member, slot)` on every slot (an empty slot records the first member: its records are never read,
+    // the slot being dead) with a recorder installed, append the argument records of each recorded launch to
+    // `host` (one contiguous array per launch, slot after slot) and, when `launch`, issue the batched launches
+    template <class F> void emit(cudaStream_t st, F fn, std::vector<unsigned char>& host, Layout& L, bool launch) {
         const size_t B = m_.size();
         std::vector<std::vector<LaunchRecord>> recs(B);
         for (size_t b = 0; b < B; b++) {
             RecordGuard guard(&recs[b], (int)B, dgemm_tile_);
-            fn(*m_[b]);
+            if (m_[b]) fn(*m_[b], (int)b);
+            else fn(*proto_, 0);
         }
         for (size_t b = 1; b < B; b++) {
             bool same = recs[b].size() == recs[0].size();
@@ -1368,8 +1480,9 @@ private:
             const size_t off = align256(host.size());
             host.resize(off + sz * B);
             for (size_t b = 0; b < B; b++) std::memcpy(host.data() + off + b * sz, recs[b][j].args.data(), sz);
-            // the work list: every cavity's blocks of its own launch grid, cavity after cavity (identical lists
-            // are stored once)
+            L.launches.push_back({recs[0][j].kind, recs[0][j].variant, recs[0][j].smem, off, sz, recs[0][j].grid});
+            // the work list: every slot's blocks of its cavity's own launch grid, slot after slot (identical
+            // lists are stored once)
             size_t items_off = 0, n_items = 0;
             if (recs[0][j].kind != kLkStepBegin) {
                 std::vector<BatchItem> items;
@@ -1393,99 +1506,120 @@ private:
             }
             if (launch)
                 launch_batched(recs[0][j], dbase + off, reinterpret_cast<const BatchItem*>(dbase + items_off),
-                               (unsigned int)n_items, (int)B, st);
+                               (unsigned int)n_items, reinterpret_cast<const int*>(dbase + L.live), (int)B, st);
         }
     }
-    void launch_batched(const LaunchRecord& r, const void* d, const BatchItem* items, unsigned int n_items, int B,
-                        cudaStream_t st) {
+    void launch_batched(const LaunchRecord& r, const void* d, const BatchItem* items, unsigned int n_items,
+                        const int* live, int B, cudaStream_t st) {
         const dim3 g(n_items);
         switch (r.kind) {
-        case kLkStepBegin: check(launch_pdl(step_begin_batched, dim3(1, 1, B), dim3(32), 0, st, (const StepBeginArgs*)d)); break;
+        case kLkStepBegin:
+            check(launch_pdl(step_begin_batched, dim3(1, 1, B), dim3(32), 0, st, (const StepBeginArgs*)d, live));
+            break;
         case kLkSweep:
             if (r.variant == kSweepMarch)
                 check(launch_pdl(sweep_march_batched<T, S_::kMarchTX, S_::kMarchTY>, g, dim3(S_::MarchG::NT), r.smem, st,
-                                 (const MomentumArgs<T>*)d, items));
+                                 (const MomentumArgs<T>*)d, items, live));
             else
                 check(launch_pdl(sweep_tile_batched<T, kTY, kTZ, kNT>, g, dim3(kNT), r.smem, st,
-                                 (const MomentumArgs<T>*)d, items));
+                                 (const MomentumArgs<T>*)d, items, live));
             break;
-        case kLkStart: check(launch_pdl(projection_start_batched<T>, g, dim3(kThreads), 0, st, (const StartArgs<T>*)d, items)); break;
-        case kLkResidual: check(launch_pdl(residual_batched, g, dim3(kThreads), 0, st, (const ResidualArgs*)d, items)); break;
-        case kLkFinish: check(launch_pdl(finish_batched<T>, g, dim3(kThreads), 0, st, (const FinishArgs<T>*)d, items)); break;
+        case kLkStart:
+            check(launch_pdl(projection_start_batched<T>, g, dim3(kThreads), 0, st, (const StartArgs<T>*)d, items, live));
+            break;
+        case kLkResidual:
+            check(launch_pdl(residual_batched, g, dim3(kThreads), 0, st, (const ResidualArgs*)d, items, live));
+            break;
+        case kLkFinish:
+            check(launch_pdl(finish_batched<T>, g, dim3(kThreads), 0, st, (const FinishArgs<T>*)d, items, live));
+            break;
         case kLkDgemm64:
-            check(launch_pdl(dgemm_mma_batched<64, 64, 2, 2, 32>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, items));
+            check(launch_pdl(dgemm_mma_batched<64, 64, 2, 2, 32>, g, dim3(128), 0, st, (const GemmArgs<double>*)d, items,
+                             live));
             break;
         case kLkDgemm32:
-            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 4, 64>, g, dim3(256), 0, st, (const GemmArgs<double>*)d, items));
+            check(launch_pdl(dgemm_mma_batched<32, 32, 2, 4, 64>, g, dim3(256), 0, st, (const GemmArgs<double>*)d, items,
+                             live));
             break;
-        case kLkTc: launch_tc_batched(r.variant, g, items, (const TcTransformArgs*)d, st); break;
+        case kLkTc: launch_tc_batched(r.variant, g, items, live, (const TcTransformArgs*)d, st); break;
         default: fail("batch: unknown launch");
         }
     }
-    // the step for state parity S (as Solver::enqueue_step); `launch` = false only records (sizes the argument
-    // buffer), true captures the batched launches into the graph being built on stream_
-    void sequence(int S, std::vector<unsigned char>& host, bool launch) {
-        const int Xs = S ^ 1, Ys = 2;
-        emit(stream_, [&](S_& s) { s.launch_step_begin(stream_); }, host, launch);
+    // the step of batch parity S (as Solver::enqueue_step, each slot at its own state parity S ^ d); `launch` =
+    // false only records (sizes the argument buffer), true captures the batched launches into the graph being
+    // built on stream_
+    void sequence(int S, std::vector<unsigned char>& host, Layout& L, bool launch) {
+        L.live = 0;
+        host.resize(align256(sizeof(int) * m_.size()));
+        for (size_t i = 0; i < m_.size(); i++) reinterpret_cast<int*>(host.data())[i] = m_[i] ? 1 : 0;
+        auto par = [&](int b) { return S ^ d_[b]; };
+        emit(stream_, [&](S_& s, int) { s.launch_step_begin(stream_); }, host, L, launch);
         for (int stage = 0; stage < 3; stage++) {
-            const int in = stage == 0 ? S : stage == 1 ? Xs : Ys;
-            const int out = stage == 1 ? Ys : Xs;
-            const int cur = stage == 1 ? Xs : Ys;
-            emit(stream_, [&](S_& s) { s.launch_momentum(stream_, stage, S, in, out); }, host, launch);
-            cudaGraphConditionalHandle h = 0;
+            emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 0); }, host, L, launch);
             cudaGraph_t g = nullptr;
             const cudaGraphNode_t* deps = nullptr;
             size_t ndeps = 0;
             cudaStreamCaptureStatus status;
             if (launch) {
                 check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
-                check(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+                check(cudaGraphConditionalHandleCreate(&handles_[S][stage], g, 0, cudaGraphCondAssignDefault));
             }
-            emit(stream_, [&](S_& s) { s.launch_start(stream_, s.M_[out], true, stage, S, cur, h, 2); }, host, launch);
+            emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 1); }, host, L, launch);
             // the first pass outside the loop (see Solver::captured_loop), then the loop
-            emit(stream_, [&](S_& s) { s.launch_pass(stream_, s.praw_, h, 2); }, host, launch);
+            emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 2); }, host, L, launch);
             if (launch) {
                 check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
                 cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
                 cp.type = cudaGraphNodeTypeConditional;
-                cp.conditional.handle = h;
+                cp.conditional.handle = handles_[S][stage];
                 cp.conditional.type = cudaGraphCondTypeWhile;
                 cp.conditional.size = 1;
                 cudaGraphNode_t node;
                 check(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
                 cudaGraph_t body = cp.conditional.phGraph_out[0];
                 check(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-                emit(body_stream_, [&](S_& s) { s.launch_pass(body_stream_, s.praw_, h, 2); }, host, launch);
+                emit(body_stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 3); }, host, L, launch);
                 check(cudaStreamEndCapture(body_stream_, &body));
                 check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
             } else {
-                emit(stream_, [&](S_& s) { s.launch_pass(stream_, s.praw_, h, 2); }, host, launch);
+                emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 3); }, host, L, launch);
             }
-            emit(stream_, [&](S_& s) { s.launch_finish(stream_, s.M_[out], s.U_[out], s.PHI_[out], true, stage, stage == 2); },
-                 host, launch);
+            emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 4); }, host, L, launch);
         }
     }
     void build(int S) {
         std::vector<unsigned char> host;
+        Layout L;
         item_lists_.clear();
-        sequence(S, host, false);
+        sequence(S, host, L, false);
         check(cudaMalloc(&dargs_[S], std::max<size_t>(host.size(), 256)));
         dargs_cur_ = dargs_[S];
         host.clear();
         item_lists_.clear();
+        layout_[S] = Layout();
         check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-        sequence(S, host, true);
+        sequence(S, host, layout_[S], true);
         check(cudaStreamEndCapture(stream_, &graph_[S]));
         check(cudaGraphInstantiate(&exec_[S], graph_[S], 0));
         check(cudaMemcpy(dargs_[S], host.data(), host.size(), cudaMemcpyHostToDevice));
+        host_[S] = std::move(host);
     }
 
-    std::vector<S_*> m_;
+    std::vector<S_*> m_;                      // slot -> cavity (nullptr: empty)
+    std::vector<int> d_;                      // slot -> its cavity's state parity relative to the batch's
+    S_* proto_ = nullptr;                     // a member, while the graphs are built
+    int par_ = 0;                             // the batch's state parity: the graph the next step launches
+    bool queued_ = false;
+    int nx_ = 0, ny_ = 0, nz_ = 0, sweep_kind_ = 0;
+    bool tc_fdm_ = false;
     cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
     cudaGraph_t graph_[2] = {nullptr, nullptr};
     cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+    cudaGraphConditionalHandle handles_[2][3] = {};
     void* dargs_[2] = {nullptr, nullptr};
     void* dargs_cur_ = nullptr;
+    std::vector<unsigned char> host_[2];      // host copies of the argument buffers
+    Layout layout_[2];
     bool mixed_sizes_ = false;
     int dgemm_tile_ = 0;
     std::map<std::string, size_t> item_lists_;      // work lists already in the argument buffer, by content
@@ -1663,7 +1797,7 @@ using cavity::SolverBase;
 struct CavitySolver { std::unique_ptr<SolverBase> s; };
 struct CavityBatch { std::unique_ptr<cavity::BatchBase> b; };
 
-static std::string g_last_error;
+static thread_local std::string g_last_error;     // per calling thread (cavities set up on a worker thread)
 static CavitySolver* g_default = nullptr;
 static int g_precision = 0;
 
@@ -1819,6 +1953,9 @@ int cavity_eigenbasis(const CavityConfig* config, int axis, int on_gpu, double* 
 }
 long long cavity_pressure_passes(const CavitySolver* s) { return s && s->s ? s->s->pressure_passes() : -1; }
 int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** out) {
+    return cavity_batch_create_slots(members, count, count, out);
+}
+int cavity_batch_create_slots(CavitySolver* const* members, int count, int capacity, CavityBatch** out) {
     return safely([&] {
         if (!members || count < 1 || !out) cavity::fail("batch: need at least one cavity");
         std::vector<cavity::Solver<double>*> d;
@@ -1830,8 +1967,8 @@ int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** o
         }
         if (!d.empty() && !f.empty()) cavity::fail("batch: every cavity needs the same precision form");
         std::unique_ptr<CavityBatch> b(new CavityBatch);
-        if (!d.empty()) b->b.reset(new cavity::Batch<double>(d));
-        else b->b.reset(new cavity::Batch<float>(f));
+        if (!d.empty()) b->b.reset(new cavity::Batch<double>(d, capacity));
+        else b->b.reset(new cavity::Batch<float>(f, capacity));
         *out = b.release();
     });
 }
@@ -1847,6 +1984,13 @@ int cavity_batch_sync(CavityBatch* b, CavityReport* reports) {
         b->b->sync(reports);
     });
 }
+int cavity_batch_set_member(CavityBatch* b, int slot, CavitySolver* s) {
+    return safely([&] {
+        if (!b || !b->b) cavity::fail("invalid batch handle");
+        b->b->set_member(slot, s ? &H(s) : nullptr);
+    });
+}
+int cavity_batch_size(const CavityBatch* b) { return b && b->b ? b->b->size() : -1; }
 int cavity_batch_destroy(CavityBatch* b) { return safely([&] { delete b; }); }
 const char* cavity_last_error(void) { return g_last_error.c_str(); }
 }

@@ -470,10 +470,11 @@ __global__ void __launch_bounds__(TX * TY, sizeof(T) == 4 ? 3 : 1) sweep_march_k
 // a batch of cavities: grid x runs over the work list (BatchItem)
 template <class T, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY, sizeof(T) == 4 ? 3 : 1)
-    sweep_march_batched(const MomentumArgs<T>* args, const BatchItem* items) {
+    sweep_march_batched(const MomentumArgs<T>* args, const BatchItem* items, const int* live) {
     __shared__ MomentumArgs<T> a;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(a, args + cav);
     sweep_march_body<T, TX, TY>(a, k);
 }

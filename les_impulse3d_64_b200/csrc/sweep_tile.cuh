@@ -380,10 +380,12 @@ __global__ void __launch_bounds__(NT) sweep_tile_kernel(MomentumArgs<T> a) {
 }
 // a batch of cavities: grid x runs over the work list (BatchItem)
 template <class T, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) sweep_tile_batched(const MomentumArgs<T>* args, const BatchItem* items) {
+__global__ void __launch_bounds__(NT) sweep_tile_batched(const MomentumArgs<T>* args, const BatchItem* items,
+                                                          const int* live) {
     __shared__ MomentumArgs<T> a;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(a, args + cav);
     sweep_tile_body<T, TY, TZ, NT>(a, k);
 }

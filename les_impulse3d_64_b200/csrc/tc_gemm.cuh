@@ -438,10 +438,12 @@ __global__ void __launch_bounds__(kTcThreads) tc_transform_kernel(TcTransformArg
 }
 // a batch of cavities: grid x runs over the work list (BatchItem)
 template <int BN, int FA, int F64>
-__global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTransformArgs* args, const BatchItem* items) {
+__global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTransformArgs* args, const BatchItem* items,
+                                                                   const int* live) {
     __shared__ TcTransformArgs g;
     int cav;
-    const Blk k = item_blk(items, cav);
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) return;
     load_args(g, args + cav);
     tc_transform_body<BN, FA, F64>(g, k, first_block());
 }
@@ -482,18 +484,19 @@ inline cudaError_t tc_transform_prepare_batched() {
     return e;
 }
 template <int BN>
-inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, const BatchItem* items, const TcTransformArgs* d,
-                                 cudaStream_t st) {
+inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, const BatchItem* items, const int* live,
+                                 const TcTransformArgs* d, cudaStream_t st) {
     const dim3 block(kTcThreads);
-    if (fa && f64) launch_pdl(tc_transform_batched<BN, 1, 1>, grid, block, TcSmem<BN>::kBytes, st, d, items);
-    else if (fa) launch_pdl(tc_transform_batched<BN, 1, 0>, grid, block, TcSmem<BN>::kBytes, st, d, items);
-    else launch_pdl(tc_transform_batched<BN, 0, 0>, grid, block, TcSmem<BN>::kBytes, st, d, items);
+    if (fa && f64) launch_pdl(tc_transform_batched<BN, 1, 1>, grid, block, TcSmem<BN>::kBytes, st, d, items, live);
+    else if (fa) launch_pdl(tc_transform_batched<BN, 1, 0>, grid, block, TcSmem<BN>::kBytes, st, d, items, live);
+    else launch_pdl(tc_transform_batched<BN, 0, 0>, grid, block, TcSmem<BN>::kBytes, st, d, items, live);
 }
 // a recorded launch (variant: see tc_variant) over a batch of cavities
-inline void launch_tc_batched(int variant, dim3 grid, const BatchItem* items, const TcTransformArgs* d, cudaStream_t st) {
+inline void launch_tc_batched(int variant, dim3 grid, const BatchItem* items, const int* live, const TcTransformArgs* d,
+                              cudaStream_t st) {
     const int bn = variant & 0xff, fa = (variant >> 8) & 1, f64 = (variant >> 9) & 1;
-    if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, items, d, st);
-    else launch_tc_batched_bn<32>(fa, f64, grid, items, d, st);
+    if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, items, live, d, st);
+    else launch_tc_batched_bn<32>(fa, f64, grid, items, live, d, st);
 }
 inline cudaError_t tc_transform_prepare() {
     cudaError_t e = tc_prepare_bn<64>();

@@ -3,12 +3,13 @@ batching, and the time-to-solution of every request.
 
 A request is a cavity (grid size, Reynolds number, lid shape) with its initial noise, to be run until its
 clock reaches `t_end`.  The server advances every running cavity `chunk` steps per round.  Running cavities of
-the same grid size are stepped as one batch (`cavity_batch_*`: one launch per kernel for all of them); a batch
-is rebuilt when a request joins or leaves its group.  While a round's steps run on the GPU, the host admits
+the same grid size share slot batches (`cavity_batch_create_slots`: one launch per kernel for all slots, one
+CUDA graph per batch built once); a request takes a free slot (`cavity_batch_set_member`) and gives it back when
+it finishes, so joining and leaving rebuild nothing.  While a round's steps run on the GPU, the host admits
 waiting requests in arrival order, as long as their estimated device bytes (`cavity_estimate_bytes`) fit in
-the budget, and sets them up (solver creation and the initial projection); they join at the next round.  A
-request finishes at the end of the first round in which its clock reaches `t_end`; its time to solution is
-that moment minus its arrival.  With `batched=False, max_running=1` the same loop serves one request at a time through its own graph
+the budget, and a set-up thread creates them and runs their initial projection on their own streams; they join
+the first round after their set-up is done.  A request finishes at the end of the first round in which its
+clock reaches `t_end`; its time to solution is that moment minus its arrival.  With `batched=False, max_running=1` the same loop serves one request at a time through its own graph
 (the plain form the batched server is compared with).
 """
 import math
@@ -84,98 +85,153 @@ class _Running:
     admitted: float
     bytes: int
     key: tuple = field(default=())
+    batch: object = None          # the slot batch it runs in (batched serving)
+    slot: int = -1
+
+
+def _set_up(request, precision, library):
+    """Create and initialise a request's cavity (runs on the set-up thread)."""
+    cav = Cavity(request.settings, precision=precision, library=library)
+    try:
+        cav.initialize(*request.initial_fields(cav.shapes))
+    except Exception:
+        cav.close()
+        raise
+    return cav
 
 
 class Server:
+    """`batched`: running cavities of one grid size share slot batches of `slots` slots (one CUDA graph per
+    batch, built once; a request takes a free slot when its set-up is done and frees it when it finishes, with no
+    graph rebuilt).  Otherwise every cavity steps through its own graphs.  `setup_threads` threads create and
+    initialise admitted requests while the GPU runs the round (0: on the serving thread)."""
+
     def __init__(self, budget_bytes=120e9, precision='mixed', chunk=8, batched=True, max_running=None,
-                 library=None):
+                 library=None, slots=8, setup_threads=1):
         self.budget = float(budget_bytes)
         self.precision = precision
         self.chunk = int(chunk)
         self.batched = batched
         self.max_running = max_running
         self.library = library
+        self.slots = int(slots)
+        self.setup_threads = int(setup_threads)
 
     def run(self, requests, on_finish=None):
         """Serve `requests` in real time; returns one Result per request, in id order.  `on_finish(request,
         cavity)`, if given, sees each cavity at its final state before it is released."""
+        from concurrent.futures import ThreadPoolExecutor
         waiting = sorted(requests, key=lambda r: r.arrival)
         running = []
-        batches = {}                  # size key -> (members' ids, Batch)
+        setting_up = []               # (request, admitted time, bytes, future or cavity)
+        batches = {}                  # size key -> [Batch]
         results = {}
         in_use = 0.0
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
+        pool = ThreadPoolExecutor(self.setup_threads) if self.setup_threads > 0 else None
+
         def admit():
             nonlocal in_use
             while waiting and waiting[0].arrival <= now():
-                if self.max_running is not None and len(running) + len(joining) >= self.max_running:
+                if self.max_running is not None and len(running) + len(setting_up) >= self.max_running:
                     return
                 req = waiting[0]
                 need = float(estimate_bytes(req.settings, self.precision, self.library))
-                if (running or joining) and in_use + need > self.budget:
+                if (running or setting_up) and in_use + need > self.budget:
                     return
                 waiting.pop(0)
-                cav = Cavity(req.settings, precision=self.precision, library=self.library)
-                cav.initialize(*req.initial_fields(cav.shapes))
-                joining.append(_Running(req, cav, now(), need, (cav.nx, cav.ny, cav.nz)))
+                job = (pool.submit(_set_up, req, self.precision, self.library) if pool
+                       else _set_up(req, self.precision, self.library))
+                setting_up.append((req, now(), need, job))
                 in_use += need
 
-        joining = []
+        def join(block):
+            """Cavities whose set-up is done start running (in slot batches when batched)."""
+            still = []
+            for req, admitted, need, job in setting_up:
+                if pool and not block and not job.done():
+                    still.append((req, admitted, need, job))
+                    continue
+                cav = job.result() if pool else job
+                r = _Running(req, cav, admitted, need, (cav.nx, cav.ny, cav.nz))
+                if self.batched:
+                    group = batches.setdefault(r.key, [])
+                    for b in group:
+                        free = b.free_slots()
+                        if free:
+                            b.set_member(free[0], cav)
+                            r.batch, r.slot = b, free[0]
+                            break
+                    else:
+                        b = Batch([cav], capacity=self.slots)
+                        group.append(b)
+                        r.batch, r.slot = b, 0
+                running.append(r)
+            setting_up[:] = still
+
         try:
-            while waiting or running or joining:
-                running += joining
-                joining = []
+            while waiting or running or setting_up:
+                join(block=not running)
                 if not running:
-                    time.sleep(max(0.0, min(waiting[0].arrival - now(), 0.05)))
+                    time.sleep(max(0.0, min(waiting[0].arrival - now(), 0.05)) if waiting else 0.0)
                     admit()
                     continue
                 # one round: every running cavity advances `chunk` steps; requests that arrive meanwhile are set up
-                # on the host (and their own streams) while the round runs, and join the next one
+                # on the set-up thread while the round runs, and join the next one
                 if self.batched:
-                    groups = {}
-                    for r in running:
-                        groups.setdefault(r.key, []).append(r)
-                    for key in list(batches):
-                        if key not in groups or batches[key][0] != [r.request.id for r in groups[key]]:
-                            batches.pop(key)[1].close()
-                    for key, members in groups.items():
-                        if key not in batches:
-                            batches[key] = ([r.request.id for r in members], Batch([r.cavity for r in members]))
-                    for _, b in batches.values():
+                    live = [b for group in batches.values() for b in group if b.cavities]
+                    for b in live:
                         b.step_async(self.chunk)
                     admit()
                     reports = {}
-                    for ids, b in batches.values():
-                        for i, rep in zip(ids, b.sync()):
-                            reports[i] = rep
+                    for b in live:
+                        for cav, rep in zip(b.slots, b.sync()):
+                            if cav is not None:
+                                reports[id(cav)] = rep
                 else:
                     for r in running:
                         r.cavity.step_async(self.chunk)
                     admit()
-                    reports = {r.request.id: r.cavity.sync() for r in running}
+                    reports = {id(r.cavity): r.cavity.sync() for r in running}
                 t_round = now()
                 still = []
                 for r in running:
-                    rep = reports[r.request.id]
+                    rep = reports[id(r.cavity)]
                     if rep['time'] >= r.request.t_end:
                         results[r.request.id] = Result(r.request.id, r.cavity.n_cell, r.request.arrival, r.admitted,
                                                        t_round, rep['steps'], rep['time'])
                         in_use -= r.bytes
-                        key = r.key
-                        if key in batches:
-                            batches.pop(key)[1].close()
+                        if r.batch is not None:
+                            r.batch.set_member(r.slot, None)
                         if on_finish is not None:
                             on_finish(r.request, r.cavity)
                         r.cavity.close()
                     else:
                         still.append(r)
                 running = still
+                # batches left empty are released
+                for key in list(batches):
+                    keep = []
+                    for b in batches[key]:
+                        if b.cavities:
+                            keep.append(b)
+                        else:
+                            b.close()
+                    batches[key] = keep
         finally:
-            for _, b in batches.values():
-                b.close()
-            for r in running + joining:
+            for group in batches.values():
+                for b in group:
+                    b.close()
+            for r in running:
                 r.cavity.close()
+            for req, admitted, need, job in setting_up:
+                try:
+                    (job.result() if pool else job).close()
+                except Exception:
+                    pass
+            if pool:
+                pool.shutdown(wait=True)
         return [results[k] for k in sorted(results)]
 
 
