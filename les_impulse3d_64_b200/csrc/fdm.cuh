@@ -147,7 +147,10 @@ __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_batched(cons
     __shared__ GemmArgs<double> g;
     int cav;
     const Blk k = item_blk(items, live, cav);
-    if (cav < 0) return;
+    if (cav < 0) {
+        dead_slot_clear(args, items);
+        return;
+    }
     load_args(g, args + cav);
     dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, k, first_block());
 }

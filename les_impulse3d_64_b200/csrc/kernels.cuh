@@ -203,6 +203,15 @@ __device__ __forceinline__ Blk item_blk(const BatchItem* items, const int* live,
     cavity = live[it.cav] ? (int)it.cav : -1;
     return {it.x, it.y, it.z, it.nx, it.ny, it.nz};
 }
+// The first transform of a pass clears the condition of the refinement loop's while-node, in the launch's first
+// block: the loop would never end without it.  When that block belongs to an empty slot it still clears: the
+// slot's argument record (a member's, written when the graph was built or the slot last held a cavity) names
+// the same loop.
+template <class A> __device__ __forceinline__ void dead_slot_clear(const A* args, const BatchItem* items) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const A& r = args[items[0].cav];
+    if (r.clear_condition) cudaGraphSetConditional(r.handle, 0u);
+}
 __device__ __forceinline__ bool first_block() { return blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0; }
 // Cells visited as columns: a block takes kThreads consecutive cells of an x-y plane (x fastest) and walks them
 // up a chunk of z-layers; grid y runs over the chunks.  A thread's plane position, and so its x and y table

@@ -443,7 +443,10 @@ __global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTrans
     __shared__ TcTransformArgs g;
     int cav;
     const Blk k = item_blk(items, live, cav);
-    if (cav < 0) return;
+    if (cav < 0) {
+        dead_slot_clear(args, items);
+        return;
+    }
     load_args(g, args + cav);
     tc_transform_body<BN, FA, F64>(g, k, first_block());
 }

@@ -58,12 +58,15 @@ def test_admission_respects_the_budget():
         assert b.admitted >= a.finished - 1e-3
 
 
-@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
-def test_slot_batch_takes_members_in_and_out(precision):
+@pytest.mark.parametrize('precision, fdm', [('fp64', 'dmma'), ('mixed', 'dmma'), ('mixed', 'tc')])
+def test_slot_batch_takes_members_in_and_out(precision, fdm, monkeypatch):
     """A batch of three slots: A starts alone in it; B, stepped once on its own (the other state parity), joins;
-    A leaves and C joins its slot.  Each cavity's state after its steps in the batch equals that of a twin stepped
-    the same number of steps alone, to rounding."""
+    A leaves, the batch steps with its first slot empty (the first block of every launch then belongs to an
+    empty slot, which must still end each refinement loop), and C joins that slot.  Each cavity's state after its
+    steps in the batch equals that of a twin stepped the same number of steps alone, to rounding.  Both transform
+    paths: FP64 DMMA, and the mixed form's tensor-core transforms (CAVITY_FDM=tc)."""
     from les_impulse3d_64_b200.api import Batch
+    monkeypatch.setenv('CAVITY_FDM', fdm)
     s = workloads.settings(24, 800.0, beta=1.5, cfl=0.5)
     tol = 1e-12 if precision == 'fp64' else 1e-6
 
@@ -84,6 +87,8 @@ def test_slot_batch_takes_members_in_and_out(precision):
         batch.step_async(3); reps = batch.sync(); steps['a'] += 3; steps['b'] += 3
         assert reps[2] is None and reps[0]['steps'] == 5 and reps[1]['steps'] == 4
         batch.set_member(0, None)
+        batch.step_async(2); reps = batch.sync(); steps['b'] += 2
+        assert reps[0] is None and reps[1]['steps'] == 6
         batch.set_member(0, c)
         batch.step_async(2); batch.sync(); steps['b'] += 2; steps['c'] += 2
         for name, cav in (('a', a), ('b', b), ('c', c)):
