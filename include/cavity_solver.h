@@ -101,14 +101,16 @@ long long cavity_estimate_bytes(const CavityConfig* config, int precision);
  * receives the device time of each one's momentum-sweep launches (see also cavity_kernel_times). */
 int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms_per_step, float* kernel_ms);
 /* Autotuner (no counterpart in the reference): times `steps` whole steps from the current state under each
- * candidate launch shape - the march sweep's z-chunk count; the FP64 transforms as six launches of 64 x 64 or
- * 32 x 32 tiles, or as one cooperative launch of 32 x 32 tiles - restoring the state after each, and keeps the
- * fastest for this cavity.  The choice is cached per
- * grid size, stretching and precision form for the process, and in the file named by CAVITY_TUNE_FILE when that
- * is set; cavities created later with the same key start with it.  No candidate changes the arithmetic: every
- * one gives bit-identical steps.  With CAVITY_AUTOTUNE=1 a cavity without a cached choice tunes itself (6 steps
- * per candidate) before its first step.  Outputs (each may be NULL): the chosen chunk count, tile (0: the
- * size rule) and one-launch choice (1 yes, 0 no, -1 the size rule), and the step time in milliseconds. */
+ * candidate, restoring the state after each, and keeps the fastest for this cavity, in two rounds: the momentum
+ * sweep (the tile kernel, or the z-march with 1/2, 1, 2 or 4 times its device-filling z-chunk count; only the
+ * kernel CAVITY_SWEEP names, when set), then the FP64 transforms (six launches of 64 x 64 or 32 x 32 tiles, or
+ * one cooperative launch of 32 x 32 tiles).  The choice is cached per grid size, stretching and precision form
+ * for the process, and in the file named by CAVITY_TUNE_FILE when that is set; cavities created later with the
+ * same key start with it.  The transform choices and the chunk counts give bit-identical steps; the two sweep
+ * kernels agree to rounding.  With CAVITY_AUTOTUNE=1 a cavity without a cached choice tunes itself (6 steps per
+ * candidate) before its first step.  Outputs (each may be NULL): the chosen chunk count (0: the tile sweep),
+ * tile (0: the size rule) and one-launch choice (1 yes, 0 no, -1 the size rule), and the step time in
+ * milliseconds. */
 int cavity_autotune(CavitySolver* s, int steps, int* march_chunks, int* dgemm_tile, int* fused_pass, float* ms_per_step);
 /* After cavity_time_steps: ms[4] receives the mean device time per timed step (milliseconds, all three stages)
  * of the momentum sweeps, the projection starts, the residuals of their warm-start guesses, and the finishes.

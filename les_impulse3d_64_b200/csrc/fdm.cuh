@@ -296,17 +296,15 @@ inline void launch_fdm_pass_fused(cudaStream_t st, const FdmOperands& op, const 
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, fdm_pass_fused_kernel, a);
 }
-// the one-launch pass applies: a single cavity (not recording a batch) whose largest transform has at most two
-// tiles per co-resident block, unless CAVITY_FDM_FUSED says otherwise (=1 always, =0 never); `want` is the
-// cavity's own choice (autotuner): -1 by the rule
+// the one-launch pass applies to a single cavity (not recording a batch) when CAVITY_FDM_FUSED=1 or the
+// cavity's own choice (`want`, the autotuner's; -1 none) says so.  It is not the default: inside the step graph
+// it measured slower than six launches (C2 step 0.383 against 0.368 ms), the graph's programmatic launches
+// already hiding most of the gaps that the grid barriers replace.
 inline bool use_fused_pass(const FdmOperands& op, int want) {
+    (void)op;
     if (g_launch_record || g_dgemm_tile == 64 || fused_pass_capacity() == 0) return false;
     if (const char* e = std::getenv("CAVITY_FDM_FUSED")) return e[0] == '1';
-    if (want >= 0) return want == 1;
-    const long long most = std::max({(long long)((op.nx + 31) / 32) * ((op.ny * op.nz + 31) / 32),
-                                     (long long)((op.nx + 31) / 32) * ((op.ny + 31) / 32) * op.nz,
-                                     (long long)((op.nx * op.ny + 31) / 32) * ((op.nz + 31) / 32)});
-    return most <= 2LL * fused_pass_capacity();
+    return want == 1;
 }
 
 inline void launch_fdm_pass(cudaStream_t st, const FdmOperands& op, const double* r, const double* r_alt, double* phi,

@@ -93,7 +93,8 @@ static long long estimate_bytes(const CavityConfig& c, int precision);
 struct Tuning {
     int chunks = 0;       // march sweep z-chunks (0: the device-filling rule)
     int dgemm = 0;        // FP64 transform tile, 32 or 64 (0: the size rule)
-    int fused = -1;       // FP64 pass as one cooperative launch: 1 yes, 0 no, -1 the size rule
+    int fused = -1;       // FP64 pass as one cooperative launch: 1 yes, 0 no, -1 not chosen
+    int sweep = -1;       // momentum sweep kernel (SweepKind; -1: not chosen)
     float ms = 0;         // measured step time of the choice
 };
 static std::string tune_key(const CavityConfig& c, int precision) {
@@ -119,7 +120,8 @@ static const Tuning* tune_lookup(const std::string& key) {
                 while (std::fgets(line, sizeof line, fp)) {
                     const char* bar = std::strchr(line, '|');
                     Tuning t;
-                    if (!bar || std::sscanf(bar + 1, "%d %d %d %f", &t.chunks, &t.dgemm, &t.fused, &t.ms) != 4) continue;
+                    if (!bar || std::sscanf(bar + 1, "%d %d %d %d %f", &t.chunks, &t.dgemm, &t.fused, &t.sweep, &t.ms) != 5)
+                        continue;
                     std::string k(line, bar - line);
                     while (!k.empty() && k.back() == ' ') k.pop_back();
                     g_tune[k] = t;
@@ -137,7 +139,7 @@ static void tune_store(const std::string& key, const Tuning& t) {
     g_tune[key] = t;
     if (const char* f = tune_file()) {
         if (FILE* fp = std::fopen(f, "a")) {
-            std::fprintf(fp, "%s | %d %d %d %.6f\n", key.c_str(), t.chunks, t.dgemm, t.fused, t.ms);
+            std::fprintf(fp, "%s | %d %d %d %d %.6f\n", key.c_str(), t.chunks, t.dgemm, t.fused, t.sweep, t.ms);
             std::fclose(fp);
         }
     }
@@ -227,6 +229,7 @@ public:
             std::lock_guard<std::mutex> lock(g_tune_mutex);
             if (const Tuning* t = tune_lookup(tune_key(c_, sizeof(T) == 8 ? 0 : 1))) tune_ = *t;
         }
+        if (tune_.sweep >= 0 && !sweep_forced_) sweep_kind_ = tune_.sweep;
         if (const char* a = std::getenv("CAVITY_AUTOTUNE")) auto_tune_ = a[0] == '1';
         check(cudaStreamSynchronize(stream_));
     }
@@ -575,9 +578,9 @@ public:
     // times come from the plain graph), for the per-kernel times
     void time_steps(int warmup, int steps, int flush, float* ms, float* kms) override {
         if (flush && !flush_) check(cudaMalloc(&flush_, kFlushBytes));
+        for (int i = 0; i < warmup; i++) step(nullptr);      // (the first may run the autotuner, which rebuilds graphs)
         ensure_graphs(false);
         if (kms) ensure_graphs(true);
-        for (int i = 0; i < warmup; i++) step(nullptr);
         for (double& t : timed_ms_) t = 0;
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0));
@@ -613,9 +616,10 @@ public:
     }
 
     // Time whole steps under each candidate launch shape from the current state, restore the state after each,
-    // and keep the fastest (cached per grid size, stretching and precision; see Tuning).  Candidates: the march
-    // sweep's z-chunk count at 1/2, 1, 2 and 4 times the device-filling count, and, where the FP64 transforms
-    // run, their 32 x 32 and 64 x 64 tiles.
+    // and keep the fastest (cached per grid size, stretching and precision; see Tuning).  Two rounds: first the
+    // momentum sweep (the tile kernel, or the march with 1/2, 1, 2 and 4 times its device-filling z-chunk count;
+    // only the chosen kernel when CAVITY_SWEEP names one), then, with the fastest sweep, the FP64 transforms where
+    // they run (64 x 64 tiles, 32 x 32 tiles, 32 x 32 tiles in one cooperative launch).
     void autotune(int steps, int* chunks_out, int* dgemm_out, int* fused_out, float* ms_out) override {
         if (!pending_.empty()) fail("autotune: steps are queued; sync first");
         steps = std::max(steps, 2);
@@ -624,62 +628,80 @@ public:
         void* saved = nullptr;
         check(cudaMalloc(&saved, (size_t)bytes));
         checkpoint_save(saved, 1);
-        tune_ = Tuning{};
-        const int c0 = (int)march_chunks();
-        std::vector<int> cands;
-        for (int c : {c0, c0 / 2, 2 * c0, 4 * c0}) {
-            c = std::min(std::max(c, 1), std::max(1, nz_ / 4));
-            if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
-        }
-        if (sweep_kind_ != kSweepMarch) cands = {0};
-        // FP64 transform variants: 64 x 64 tiles, 32 x 32 tiles, and 32 x 32 tiles in one cooperative launch
-        std::vector<std::pair<int, int>> tiles = {{0, -1}};
-        if (!tc_fdm_) {
-            tiles = {{64, 0}, {32, 0}};
-            if (fused_pass_capacity() > 0) tiles.push_back({32, 1});
-        }
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0));
         check(cudaEventCreate(&e1));
+        auto time_candidate = [&](const Tuning& cand) {
+            tune_ = cand;
+            if (cand.sweep >= 0) sweep_kind_ = cand.sweep;
+            drop_graphs();
+            float ms = -1;
+            try {
+                ensure_graphs(false);
+                step(nullptr);                                   // warm-up (graph upload)
+                check(cudaEventRecord(e0, stream_));
+                for (int i = 0; i < steps; i++) {
+                    check(cudaGraphLaunch(exec_[par_], stream_));
+                    pending_.push_back(par_);
+                    par_ ^= 1;
+                }
+                check(cudaEventRecord(e1, stream_));
+                sync(nullptr);
+                check(cudaEventElapsedTime(&ms, e0, e1));
+                ms /= steps;
+            } catch (const std::exception&) {
+                ms = -1;                                         // a failed step: not a candidate
+            }
+            pending_.clear();
+            checkpoint_load(saved, 1);
+            return ms;
+        };
         Tuning best;
         best.ms = -1;
-        for (int c : cands)
+        auto consider = [&](const Tuning& cand) {
+            const float ms = time_candidate(cand);
+            if (ms > 0 && (best.ms < 0 || ms < best.ms)) {
+                best = cand;
+                best.ms = ms;
+            }
+        };
+        // round 1: the sweep
+        const int forced = sweep_forced_ ? sweep_kind_ : -1;
+        std::vector<Tuning> sweeps;
+        if (forced < 0 || forced == kSweepTile) sweeps.push_back(Tuning{0, 0, -1, kSweepTile, 0});
+        if (forced < 0 || forced == kSweepMarch) {
+            const int kind = sweep_kind_;
+            sweep_kind_ = kSweepMarch;
+            tune_ = Tuning{};
+            const int c0 = (int)march_chunks();
+            sweep_kind_ = kind;
+            std::vector<int> cs;
+            for (int c : {c0, c0 / 2, 2 * c0, 4 * c0}) {
+                c = std::min(std::max(c, 1), std::max(1, nz_ / 4));
+                if (std::find(cs.begin(), cs.end(), c) == cs.end()) cs.push_back(c);
+            }
+            for (int c : cs) sweeps.push_back(Tuning{c, 0, -1, kSweepMarch, 0});
+        }
+        if (forced == kSweepFace) sweeps.push_back(Tuning{0, 0, -1, kSweepFace, 0});
+        for (const Tuning& t : sweeps) consider(t);
+        // round 2: the FP64 transforms, with that sweep
+        if (!tc_fdm_ && best.ms > 0) {
+            std::vector<std::pair<int, int>> tiles = {{64, 0}, {32, 0}};
+            if (fused_pass_capacity() > 0) tiles.push_back({32, 1});
+            const Tuning sw = best;
             for (const auto& t : tiles) {
-                Tuning cand;
-                cand.chunks = c;
+                Tuning cand = sw;
                 cand.dgemm = t.first;
                 cand.fused = t.second;
-                tune_ = cand;
-                drop_graphs();
-                float ms = -1;
-                try {
-                    ensure_graphs(false);
-                    step(nullptr);                                   // warm-up (graph upload)
-                    check(cudaEventRecord(e0, stream_));
-                    for (int i = 0; i < steps; i++) {
-                        check(cudaGraphLaunch(exec_[par_], stream_));
-                        pending_.push_back(par_);
-                        par_ ^= 1;
-                    }
-                    check(cudaEventRecord(e1, stream_));
-                    sync(nullptr);
-                    check(cudaEventElapsedTime(&ms, e0, e1));
-                    ms /= steps;
-                } catch (const std::exception&) {
-                    ms = -1;                                         // a failed step: not a candidate
-                }
-                pending_.clear();
-                checkpoint_load(saved, 1);
-                if (ms > 0 && (best.ms < 0 || ms < best.ms)) {
-                    best = cand;
-                    best.ms = ms;
-                }
+                consider(cand);
             }
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaFree(saved);
         if (best.ms < 0) best = Tuning{};
         tune_ = best;
+        if (best.sweep >= 0) sweep_kind_ = best.sweep;
         drop_graphs();
         if (best.ms > 0) tune_store(tune_key(c_, sizeof(T) == 8 ? 0 : 1), best);
         if (chunks_out) *chunks_out = best.chunks;
@@ -1110,11 +1132,10 @@ private:
             const char* sw = std::getenv("CAVITY_SWEEP");
             const std::string kind = sw ? sw : "";
             sweep_kind_ = kind == "face" ? kSweepFace : kind == "march" ? kSweepMarch : kSweepTile;
-            if (sweep_kind_ == kSweepTile)
-                check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)TileG::template smem_bytes<T>()));
-            if (sweep_kind_ == kSweepMarch) {
+            sweep_forced_ = !kind.empty();
+            check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TileG::template smem_bytes<T>()));
+            {
                 const int smem = (int)MarchG::template smem_bytes<T>();
                 check(cudaFuncSetAttribute(sweep_march_kernel<T, kMarchTX, kMarchTY>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -1190,6 +1211,7 @@ private:
     int par_ = 0;
     bool eager_ = false;
     int sweep_kind_ = kSweepTile;
+    bool sweep_forced_ = false;         // CAVITY_SWEEP named the kernel
     Tuning tune_;
     bool auto_tune_ = false;
     int march_per_sm_ = 1;

@@ -71,21 +71,6 @@ template <int TX_, int TY_> struct MarchGeom {
 
 __device__ __forceinline__ int ring(int layer, int slots) { return (layer + 60) % slots; }
 
-// Stage one layer (W x H box, corner (xs, ys)) of an array with extents (ex, ey, ez) into shared memory;
-// elements outside the array are zero.
-template <class T, int W, int H, int NT>
-__device__ __forceinline__ void stage_layer(T* dst, const T* __restrict__ src, int xs, int ys, int layer, int ex, int ey,
-                                            int ez) {
-    const bool zin = layer >= 0 && layer < ez;
-    const T* lay = src + (size_t)(zin ? layer : 0) * (size_t)ex * (size_t)ey;
-    for (int e = threadIdx.x; e < W * H; e += NT) {
-        const int row = e / W, col = e - row * W;
-        const int gx = xs + col, gy = ys + row;
-        const bool ok = zin && (unsigned)gx < (unsigned)ex && (unsigned)gy < (unsigned)ey;
-        cp_async_zfill<sizeof(T)>(dst + e, ok ? lay + gx + (size_t)gy * ex : src, ok);
-    }
-}
-
 // coefficients of an edge position along one axis (index i of faces along that axis)
 template <class T> struct EdgeCoef {
     T ok1, l1, isp, l3, ind3, e1l, e1h, e3l, e3h;
@@ -108,31 +93,50 @@ template <class T> struct EdgeTerms {
     T g1, g3;      // second family (zV, yW, xW)
 };
 
-// Shared-memory layout and rings of one CTA
-template <class T, class G> struct MarchSmem {
-    T* base;
-    __device__ __forceinline__ T* u(int layer) const { return base + G::OU + ring(layer, G::SU) * G::NU; }
-    __device__ __forceinline__ T* v(int layer) const { return base + G::OV + ring(layer, G::SU) * G::NV; }
-    __device__ __forceinline__ T* w(int face) const { return base + G::OW + ring(face, G::SW) * G::NW; }
-    __device__ __forceinline__ T* m(int c, int layer) const { return base + G::OM + (c * G::SM + ring(layer, G::SM)) * G::NM; }
-    __device__ __forceinline__ T* k(int layer) const { return base + G::OK + ring(layer, G::SK) * G::NK; }
-    __device__ __forceinline__ T* zu1() const { return base + G::OZU; }
-    __device__ __forceinline__ T* zu3() const { return base + G::OZU + G::NZU; }
-    __device__ __forceinline__ T* zv1() const { return base + G::OZV; }
-    __device__ __forceinline__ T* zv3() const { return base + G::OZV + G::NZV; }
-    __device__ __forceinline__ T* yw(int face) const { return base + G::OYW + ring(face, G::SE) * 2 * G::NYW; }
-    __device__ __forceinline__ T* xw(int face) const { return base + G::OXW + ring(face, G::SE) * 2 * G::NXW; }
+// Stage rows of one layer of an array with extents (ex, ey, ez) into a W x H box (corner xs, ys) in shared memory,
+// a warp per row (rows warp, warp + WARPS, ...) and a lane per column (lane, lane + 32; W <= 64); elements outside
+// the array are zero.
+template <class T, int W, int H, int WARPS>
+__device__ __forceinline__ void stage_rows(T* dst, const T* __restrict__ src, int xs, int ys, int layer, int ex, int ey,
+                                           int ez, int lane, int warp) {
+    static_assert(W <= 64, "two columns per lane");
+    const bool zin = layer >= 0 && layer < ez;
+    const T* lay = src + (zin ? (size_t)layer * (size_t)ex * (size_t)ey : (size_t)0);
+    const int gx0 = xs + lane, gx1 = xs + lane + 32;
+    const bool ok0 = zin && (unsigned)gx0 < (unsigned)ex;
+    const bool ok1 = lane + 32 < W && zin && (unsigned)gx1 < (unsigned)ex;
+    for (int r = warp; r < H; r += WARPS) {
+        const int gy = ys + r;
+        const bool yok = (unsigned)gy < (unsigned)ey;
+        const T* row = lay + (size_t)(yok ? gy : 0) * (size_t)ex;
+        T* d = dst + r * W;
+        cp_async_zfill<sizeof(T)>(d + lane, ok0 && yok ? row + gx0 : src, ok0 && yok);
+        if (lane + 32 < W) cp_async_zfill<sizeof(T)>(d + lane + 32, ok1 && yok ? row + gx1 : src, ok1 && yok);
+    }
+}
+
+__device__ __forceinline__ int wrap(int v, int slots) { return v >= slots ? v - slots : v; }
+
+// the face coefficients of one axis at index i: 1/width at i and i-1, 1/spacing at i and i+1, the wide-stencil
+// weight at i (the viscous flux Laplacian's and the Lamb sum's tables)
+template <class T> struct FaceCoef {
+    T iw0, iwm, is0, is1, c3;
 };
+template <class T> __device__ __forceinline__ FaceCoef<T> face_coef(const Geo<T>& g, int a, int i, int n) {
+    const int c = min(max(i, -1), n + 1);
+    return {tab(g, a, kInvW, c), tab(g, a, kInvW, c - 1), tab(g, a, kInvSp, c), tab(g, a, kInvSp, c + 1), tab(g, a, kC3, c)};
+}
 
 template <class T, int TX, int TY>
 __device__ void sweep_march_body(const MomentumArgs<T>& a, const Blk& blk) {
+    static_assert(TX == 32 && TY == 8, "a warp per row of a 32 x 8 column block; the halo tasks are laid out for 8 warps");
     using G = MarchGeom<TX, TY>;
-    constexpr int NT = G::NT, UW = G::UW, VW = G::VW, WW = G::WW, MW = G::MW, KW = G::KW;
+    constexpr int UW = G::UW, VW = G::VW, WW = G::WW, MW = G::MW, KW = G::KW, EW = TX + 3;
     pdl_launch_dependents();
     pdl_wait();
     if (a.c->error) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const MarchSmem<T, G> S{reinterpret_cast<T*>(smem_raw)};
+    T* const base = reinterpret_cast<T*>(smem_raw);
     const Params& p = a.p;
     const Geo<T>& g = a.g;
     const int nx = p.nx, ny = p.ny, nz = p.nz, o4 = p.o4;
@@ -141,74 +145,66 @@ __device__ void sweep_march_body(const MomentumArgs<T>& a, const Blk& blk) {
     const int z0 = (int)blk.z * zc, z1 = min(nz, z0 + zc);
     if (z0 >= z1) return;
     const bool blend = a.stage == 0;
-    const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-    const int x = x0 + tx, y = y0 + ty;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = x0 + lane, y = y0 + warp;
     const bool live = x < nx && y < ny;
+    const T half = T(0.5);
 
-    // ---- staging of the layers one iteration needs next: u, v (layer j+4), w (z-face j+3), impulse (j+2)
-    auto stage_uv = [&](int l) {
-        stage_layer<T, G::UW, G::UH, NT>(S.u(l), a.u[X], x0 - 1, y0 - 3, l, nx + 1, ny, nz);
-        stage_layer<T, G::VW, G::VH, NT>(S.v(l), a.u[Y], x0 - 3, y0 - 1, l, nx, ny + 1, nz);
-    };
-    auto stage_w = [&](int l) { stage_layer<T, G::WW, G::WH, NT>(S.w(l), a.u[Z], x0 - 3, y0 - 3, l, nx, ny, nz + 1); };
-    auto stage_m = [&](int l) {
-        stage_layer<T, G::MW, G::MH, NT>(S.m(X, l), a.m[X], x0 - 1, y0 - 1, l, nx + 1, ny, nz);
-        stage_layer<T, G::MW, G::MH, NT>(S.m(Y, l), a.m[Y], x0 - 1, y0 - 1, l, nx, ny + 1, nz);
-        stage_layer<T, G::MW, G::MH, NT>(S.m(Z, l), a.m[Z], x0 - 1, y0 - 1, l, nx, ny, nz + 1);
-    };
-    // the gauge-reset blend of a staged impulse layer (stage 0), in place, from the staged velocity
-    auto blend_m = [&](int l) {
-        T* mu = S.m(X, l);
-        T* mv = S.m(Y, l);
-        T* mw = S.m(Z, l);
-        const T* su = S.u(l);
-        const T* sv = S.v(l);
-        const T* sw = S.w(l);
-        for (int e = threadIdx.x; e < G::NM; e += NT) {
-            const int row = e / MW, col = e - row * MW;
-            mu[e] = a.r * mu[e] + a.one_minus_r * su[(row + 2) * UW + col];
-            mv[e] = a.r * mv[e] + a.one_minus_r * sv[row * VW + col + 2];
-            mw[e] = a.r * mw[e] + a.one_minus_r * sw[(row + 2) * WW + col + 2];
+    // ring slots (see MarchGeom): offsets of layer/face j + k given the slot of j
+    auto U = [&](int su, int k) { return base + G::OU + wrap(su + k, G::SU) * G::NU; };
+    auto V = [&](int su, int k) { return base + G::OV + wrap(su + k, G::SU) * G::NV; };
+    auto Wf = [&](int sw, int k) { return base + G::OW + wrap(sw + k, G::SW) * G::NW; };
+    auto M = [&](int c, int sm, int k) { return base + G::OM + (c * G::SM + wrap(sm + k, G::SM)) * G::NM; };
+    auto stage = [&](int su, int sw, int sm, int lu, int lw, int lm, bool uv, bool w, bool m) {
+        if (uv) {
+            stage_rows<T, G::UW, G::UH, TY>(U(su, 0), a.u[X], x0 - 1, y0 - 3, lu, nx + 1, ny, nz, lane, warp);
+            stage_rows<T, G::VW, G::VH, TY>(V(su, 0), a.u[Y], x0 - 3, y0 - 1, lu, nx, ny + 1, nz, lane, warp);
+        }
+        if (w) stage_rows<T, G::WW, G::WH, TY>(Wf(sw, 0), a.u[Z], x0 - 3, y0 - 3, lw, nx, ny, nz + 1, lane, warp);
+        if (m) {
+            stage_rows<T, G::MW, G::MH, TY>(M(X, sm, 0), a.m[X], x0 - 1, y0 - 1, lm, nx + 1, ny, nz, lane, warp);
+            stage_rows<T, G::MW, G::MH, TY>(M(Y, sm, 0), a.m[Y], x0 - 1, y0 - 1, lm, nx, ny + 1, nz, lane, warp);
+            stage_rows<T, G::MW, G::MH, TY>(M(Z, sm, 0), a.m[Z], x0 - 1, y0 - 1, lm, nx, ny, nz + 1, lane, warp);
         }
     };
 
-    // ---- edges.  Smem views: U(a, b) of layer l at (b - y0 + 3) * UW + a - x0 + 1; V(a, b) at
+    // ---- edges, from the staged boxes: U(a, b) at (b - y0 + 3) * UW + a - x0 + 1; V(a, b) at
     // (b - y0 + 1) * VW + a - x0 + 3; W(a, b) at (b - y0 + 3) * WW + a - x0 + 3.
-    const T half = T(0.5);
-    // z-edge (x-face ea, y-face eb) of layer l: f = zU, g = zV (backend.cu:141-146, 177-194)
-    auto z_edge = [&](int ea, int eb, int l, const EdgeCoef<T>& cx, const EdgeCoef<T>& cy) {
-        const T* su = S.u(l) + (eb - y0 + 3) * UW + ea - x0 + 1;
-        const T* sv = S.v(l) + (eb - y0 + 1) * VW + ea - x0 + 3;
+    // z-edge (x-face ea, y-face eb) of the layer in su0/sv0: f = zU, g = zV (backend.cu:141-146, 177-194)
+    auto z_edge = [&](const T* ul, const T* vl_, int ea, int eb, const EdgeCoef<T>& cx, const EdgeCoef<T>& cy) {
+        const T* su = ul + (eb - y0 + 3) * UW + ea - x0 + 1;
+        const T* sv = vl_ + (eb - y0 + 1) * VW + ea - x0 + 3;
         EdgeTerms<T> r;
         {
-            const T vl = sv[-1], vh = sv[0], ul = su[-UW], uh = su[0];
-            const T wo = march_w1<T>(o4, cx.ok1, cy.ok1, cx.l1, cy.l1) * ((vh - vl) * cx.isp - (uh - ul) * cy.isp);
+            const T vl = sv[-1], vh = sv[0], ul1 = su[-UW], uh = su[0];
+            const T wo = march_w1<T>(o4, cx.ok1, cy.ok1, cx.l1, cy.l1) * ((vh - vl) * cx.isp - (uh - ul1) * cy.isp);
             r.f1 = wo * (cx.e1l * vl + cx.e1h * vh);
-            r.g1 = -(wo * (cy.e1l * ul + cy.e1h * uh));
+            r.g1 = -(wo * (cy.e1l * ul1 + cy.e1h * uh));
         }
         if (o4) {
-            const T vl = sv[-2], vh = sv[1], ul = su[-2 * UW], uh = su[UW];
-            const T wo = march_w3<T>(cx.l3, cy.l3) * ((vh - vl) * cx.ind3 - (uh - ul) * cy.ind3);
+            const T vl = sv[-2], vh = sv[1], ul3 = su[-2 * UW], uh = su[UW];
+            const T wo = march_w3<T>(cx.l3, cy.l3) * ((vh - vl) * cx.ind3 - (uh - ul3) * cy.ind3);
             r.f3 = wo * (cx.e3l * vl + cx.e3h * vh);
-            r.g3 = -(wo * (cy.e3l * ul + cy.e3h * uh));
+            r.g3 = -(wo * (cy.e3l * ul3 + cy.e3h * uh));
         } else {
             r.f3 = r.g3 = T(0);
         }
         return r;
     };
-    // y-edge (x-face ea, cell cy, z-face e): f = yU, g = yW (backend.cu:153-158, 201-214)
-    auto y_edge = [&](int ea, int cyy, int e, const EdgeCoef<T>& cx, const EdgeCoef<T>& cz) {
+    // y-edge (x-face ea, cell cyy) of z-face plane e: u of layers e-2 .. e+1 in u4[0..3], w of plane e in
+    // wp: f = yU, g = yW (backend.cu:153-158, 201-214)
+    auto y_edge = [&](const T* const u4[4], const T* wp, int ea, int cyy, const EdgeCoef<T>& cx, const EdgeCoef<T>& cz) {
         const int ou = (cyy - y0 + 3) * UW + ea - x0 + 1;
-        const T* sw = S.w(e) + (cyy - y0 + 3) * WW + ea - x0 + 3;
+        const T* sw = wp + (cyy - y0 + 3) * WW + ea - x0 + 3;
         EdgeTerms<T> r;
         {
-            const T ul = S.u(e - 1)[ou], uh = S.u(e)[ou], wl = sw[-1], wh = sw[0];
+            const T ul = u4[1][ou], uh = u4[2][ou], wl = sw[-1], wh = sw[0];
             const T wo = march_w1<T>(o4, cz.ok1, cx.ok1, cz.l1, cx.l1) * ((uh - ul) * cz.isp - (wh - wl) * cx.isp);
             r.f1 = -(wo * (cx.e1l * wl + cx.e1h * wh));
             r.g1 = wo * (cz.e1l * ul + cz.e1h * uh);
         }
         if (o4) {
-            const T ul = S.u(e - 2)[ou], uh = S.u(e + 1)[ou], wl = sw[-2], wh = sw[1];
+            const T ul = u4[0][ou], uh = u4[3][ou], wl = sw[-2], wh = sw[1];
             const T wo = march_w3<T>(cz.l3, cx.l3) * ((uh - ul) * cz.ind3 - (wh - wl) * cx.ind3);
             r.f3 = -(wo * (cx.e3l * wl + cx.e3h * wh));
             r.g3 = wo * (cz.e3l * ul + cz.e3h * uh);
@@ -217,19 +213,20 @@ __device__ void sweep_march_body(const MomentumArgs<T>& a, const Blk& blk) {
         }
         return r;
     };
-    // x-edge (cell cx, y-face eb, z-face e): f = xV, g = xW (backend.cu:147-152, 195-200)
-    auto x_edge = [&](int cxx, int eb, int e, const EdgeCoef<T>& cy, const EdgeCoef<T>& cz) {
+    // x-edge (cell cxx, y-face eb) of z-face plane e: v of layers e-2 .. e+1 in v4[0..3]: f = xV, g = xW
+    // (backend.cu:147-152, 195-200)
+    auto x_edge = [&](const T* const v4[4], const T* wp, int cxx, int eb, const EdgeCoef<T>& cy, const EdgeCoef<T>& cz) {
         const int ov = (eb - y0 + 1) * VW + cxx - x0 + 3;
-        const T* sw = S.w(e) + (eb - y0 + 3) * WW + cxx - x0 + 3;
+        const T* sw = wp + (eb - y0 + 3) * WW + cxx - x0 + 3;
         EdgeTerms<T> r;
         {
-            const T wl = sw[-WW], wh = sw[0], vl = S.v(e - 1)[ov], vh = S.v(e)[ov];
+            const T wl = sw[-WW], wh = sw[0], vl = v4[1][ov], vh = v4[2][ov];
             const T wo = march_w1<T>(o4, cy.ok1, cz.ok1, cy.l1, cz.l1) * ((wh - wl) * cy.isp - (vh - vl) * cz.isp);
             r.f1 = wo * (cy.e1l * wl + cy.e1h * wh);
             r.g1 = -(wo * (cz.e1l * vl + cz.e1h * vh));
         }
         if (o4) {
-            const T wl = sw[-2 * WW], wh = sw[WW], vl = S.v(e - 2)[ov], vh = S.v(e + 1)[ov];
+            const T wl = sw[-2 * WW], wh = sw[WW], vl = v4[0][ov], vh = v4[3][ov];
             const T wo = march_w3<T>(cy.l3, cz.l3) * ((wh - wl) * cy.ind3 - (vh - vl) * cz.ind3);
             r.f3 = wo * (cy.e3l * wl + cy.e3h * wh);
             r.g3 = -(wo * (cz.e3l * vl + cz.e3h * vh));
@@ -238,205 +235,230 @@ __device__ void sweep_march_body(const MomentumArgs<T>& a, const Blk& blk) {
         }
         return r;
     };
-    // K = u.m of cell (cx, cy) in layer l (cx >= x0-1, cy >= y0-1)
-    auto k_cell = [&](int cx, int cy, int l) {
-        const T* su = S.u(l) + (cy - y0 + 3) * UW + cx - x0 + 1;
-        const T* sv = S.v(l) + (cy - y0 + 1) * VW + cx - x0 + 3;
+    // K = u.m of cell (cx, cy) of a layer (u, v boxes ul, vl; w boxes of its two z-faces; impulse boxes)
+    auto k_cell = [&](const T* ul, const T* vl, const T* w0, const T* w1, const T* mx, const T* my, const T* mz0,
+                      const T* mz1, int cx, int cy) {
+        const T* su = ul + (cy - y0 + 3) * UW + cx - x0 + 1;
+        const T* sv = vl + (cy - y0 + 1) * VW + cx - x0 + 3;
         const int ow = (cy - y0 + 3) * WW + cx - x0 + 3;
         const int om = (cy - y0 + 1) * MW + cx - x0 + 1;
-        const T* mx = S.m(X, l) + om;
-        const T* my = S.m(Y, l) + om;
-        return half * ((su[0] * mx[0] + su[1] * mx[1]) + (sv[0] * my[0] + sv[VW] * my[MW]) +
-                       (S.w(l)[ow] * S.m(Z, l)[om] + S.w(l + 1)[ow] * S.m(Z, l + 1)[om]));
+        return half * ((su[0] * mx[om] + su[1] * mx[om + 1]) + (sv[0] * my[om] + sv[VW] * my[om + MW]) +
+                       (w0[ow] * mz0[om] + w1[ow] * mz1[om]));
     };
 
-    // ---- the march.  Iteration j computes the y- and x-edges of z-face plane j+2 and, once j reaches the chunk,
-    // K of layer j (from j = z0-1), the z-edges of layer j and the faces of layer j.
-    for (int l = z0 - 3; l <= z0; l++) stage_uv(l);
-    for (int l = z0 - 3; l <= z0 - 1; l++) stage_w(l);
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
-
-    // the yU / xV terms of this thread's own column along z: [0] plane j-1, [1] j, [2] j+1 (after the shift)
-    T yu1_0 = T(0), yu1_1 = T(0), yu3_m1 = T(0), yu3_0 = T(0), yu3_1 = T(0);
-    T xv1_0 = T(0), xv1_1 = T(0), xv3_m1 = T(0), xv3_0 = T(0), xv3_1 = T(0);
-    // this thread's own x-face x and y-face y coefficients stay in registers for the whole march
-    const EdgeCoef<T> cx_own = edge_coef(g, X, x, nx), cy_own = edge_coef(g, Y, y, ny);
+    // ---- this thread's coefficients: its x-face x and y-face y for the edges, and its faces' tables
+    const EdgeCoef<T> cxo = edge_coef(g, X, x, nx), cyo = edge_coef(g, Y, y, ny);
+    const FaceCoef<T> fx = face_coef(g, X, x, nx), fy = face_coef(g, Y, y, ny);
     const StageConst sc = stage_const(a.stage, a.c);
     const T dt = (T)a.c->dt;
     const T lidv = (T)lid_speed(p, sc.tau);
+    const T a0 = T(sc.a0), b0 = T(sc.b), nu = a.nu;
+
+    // ---- the march.  Iteration j computes the y- and x-edges of z-face plane j+2 and, once j reaches the chunk,
+    // K of layer j (from j = z0-1), the z-edges of layer j and the faces of layer j.  Before the first: u, v of
+    // layers z0-3 .. z0 and w of z-faces z0-3 .. z0-1.
+    {
+        const int su = ring(z0 - 3, G::SU), sw = ring(z0 - 3, G::SW);
+        for (int k = 0; k < 4; k++) stage(wrap(su + k, G::SU), 0, 0, z0 - 3 + k, 0, 0, true, false, false);
+        for (int k = 0; k < 3; k++) stage(0, wrap(sw + k, G::SW), 0, 0, z0 - 3 + k, 0, false, true, false);
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+
+    // the yU / xV terms of this thread's own column along z (planes j, j+1; wide: j-1 .. j+1)
+    T yu1_0 = T(0), yu1_1 = T(0), yu3_m1 = T(0), yu3_0 = T(0), yu3_1 = T(0);
+    T xv1_0 = T(0), xv1_1 = T(0), xv3_m1 = T(0), xv3_0 = T(0), xv3_1 = T(0);
 
 #pragma unroll 1
     for (int j = z0 - 3; j < z1; j++) {
-        if (j + 1 < z1) {
-            stage_uv(j + 4);
-            stage_w(j + 3);
-            stage_m(j + 2);
-        }
+        const int su = ring(j, G::SU), sw = ring(j, G::SW), sm = ring(j - 1, G::SM), se = ring(j, G::SE);
+        const int sk = ring(j, G::SK);
+        if (j + 1 < z1) stage(wrap(su + 4, G::SU), wrap(sw + 3, G::SW), wrap(sm + 3, G::SM), j + 4, j + 3, j + 2, true, true,
+                              true);
         asm volatile("cp.async.commit_group;\n" ::: "memory");
+        const T* const u4[4] = {U(su, 0), U(su, 1), U(su, 2), U(su, 3)};
+        const T* const v4[4] = {V(su, 0), V(su, 1), V(su, 2), V(su, 3)};
+        const T* const w0 = Wf(sw, 0);             // z-face j
+        const T* const w1 = Wf(sw, 1);             // z-face j+1
+        const T* const w2 = Wf(sw, 2);             // z-face j+2 (this iteration's edge plane)
+        T* const mnext[3] = {M(X, sm, 2), M(Y, sm, 2), M(Z, sm, 2)};     // layer (z-face) j+1
         if (blend && j + 1 >= z0 - 1) {
-            blend_m(j + 1);          // arrived at the end of the previous iteration
+            // the gauge-reset blend of the impulse layer j+1 that arrived last iteration, from u, v, w of j+1
+            for (int r = warp; r < G::MH; r += TY) {
+                for (int c = lane; c < MW; c += 32) {
+                    const int e = r * MW + c;
+                    mnext[X][e] = a.r * mnext[X][e] + a.one_minus_r * u4[1][(r + 2) * UW + c];
+                    mnext[Y][e] = a.r * mnext[Y][e] + a.one_minus_r * v4[1][r * VW + c + 2];
+                    mnext[Z][e] = a.r * mnext[Z][e] + a.one_minus_r * w1[(r + 2) * WW + c + 2];
+                }
+            }
             __syncthreads();
         }
         const int e = j + 2;
-        const EdgeCoef<T> cz_e = edge_coef(g, Z, e, nz);
-        // phase A: own edges, then the halo tasks
-        const EdgeTerms<T> ye = y_edge(x, y, e, cx_own, cz_e);
-        const EdgeTerms<T> xe = x_edge(x, y, e, cy_own, cz_e);
-        S.yw(e)[ty * (TX + 3) + tx + 1] = ye.g1;
-        S.yw(e)[G::NYW + ty * (TX + 3) + tx + 1] = ye.g3;
-        S.xw(e)[(ty + 1) * TX + tx] = xe.g1;
-        S.xw(e)[G::NXW + (ty + 1) * TX + tx] = xe.g3;
-        const bool faces = j >= z0;
+        const EdgeCoef<T> cze = edge_coef(g, Z, e, nz);
+        T* const yw = base + G::OYW + wrap(se + 2, G::SE) * 2 * G::NYW;     // plane j+2
+        T* const xw = base + G::OXW + wrap(se + 2, G::SE) * 2 * G::NXW;
+        T* const kj = base + G::OK + sk * G::NK;
+        const bool faces = j >= z0, kk = j >= z0 - 1;
+        // ---- phase A: this thread's own edges and K
+        const EdgeTerms<T> ye = y_edge(u4, w2, x, y, cxo, cze);
+        const EdgeTerms<T> xe = x_edge(v4, w2, x, y, cyo, cze);
+        yw[warp * EW + lane + 1] = ye.g1;
+        yw[G::NYW + warp * EW + lane + 1] = ye.g3;
+        xw[(warp + 1) * TX + lane] = xe.g1;
+        xw[G::NXW + (warp + 1) * TX + lane] = xe.g3;
+        T* const zu = base + G::OZU;
+        T* const zv = base + G::OZV;
         if (faces) {
-            const EdgeTerms<T> ze = z_edge(x, y, j, cx_own, cy_own);
-            S.zu1()[(ty + 1) * TX + tx] = ze.f1;
-            S.zu3()[(ty + 1) * TX + tx] = ze.f3;
-            S.zv1()[ty * (TX + 3) + tx + 1] = ze.g1;
-            S.zv3()[ty * (TX + 3) + tx + 1] = ze.g3;
+            const EdgeTerms<T> ze = z_edge(u4[0], v4[0], x, y, cxo, cyo);
+            zu[(warp + 1) * TX + lane] = ze.f1;
+            zu[G::NZU + (warp + 1) * TX + lane] = ze.f3;
+            zv[warp * EW + lane + 1] = ze.g1;
+            zv[G::NZV + warp * EW + lane + 1] = ze.g3;
         }
-        if (j >= z0 - 1) S.k(j)[(ty + 1) * KW + tx + 1] = k_cell(x, y, j);
-        for (int t = threadIdx.x; t < G::HALO; t += NT) {
-            int r = t;
-            if (r < G::H_YE) {                       // y-edges at x-faces x0-1, x0+TX, x0+TX+1
-                const int c = r / TY, cy = y0 + r % TY;
-                const int col = c == 0 ? 0 : TX + c;     // box column (x-face x0-1+col)
-                const EdgeTerms<T> h = y_edge(x0 - 1 + col, cy, e, edge_coef(g, X, x0 - 1 + col, nx), cz_e);
-                S.yw(e)[(cy - y0) * (TX + 3) + col] = h.g1;
-                S.yw(e)[G::NYW + (cy - y0) * (TX + 3) + col] = h.g3;
-                continue;
+        const T* const mj[3] = {M(X, sm, 1), M(Y, sm, 1), M(Z, sm, 1)};        // layer (z-face) j
+        if (kk) {
+            kj[(warp + 1) * KW + lane + 1] = k_cell(u4[0], v4[0], w0, w1, mj[X], mj[Y], mj[Z], mnext[Z], x, y);
+            if (warp == 0)       // the row below the block
+                kj[lane + 1] = k_cell(u4[0], v4[0], w0, w1, mj[X], mj[Y], mj[Z], mnext[Z], x, y0 - 1);
+            if (lane == 0) {     // the column left of the block (and its corner)
+                kj[(warp + 1) * KW] = k_cell(u4[0], v4[0], w0, w1, mj[X], mj[Y], mj[Z], mnext[Z], x0 - 1, y);
+                if (warp == 0) kj[0] = k_cell(u4[0], v4[0], w0, w1, mj[X], mj[Y], mj[Z], mnext[Z], x0 - 1, y0 - 1);
             }
-            r -= G::H_YE;
-            if (r < G::H_XE) {                       // x-edges at y-faces y0-1, y0+TY, y0+TY+1
-                const int c = r / TX, cx = x0 + r % TX;
-                const int row = c == 0 ? 0 : TY + c;
-                const EdgeTerms<T> h = x_edge(cx, y0 - 1 + row, e, edge_coef(g, Y, y0 - 1 + row, ny), cz_e);
-                S.xw(e)[row * TX + cx - x0] = h.g1;
-                S.xw(e)[G::NXW + row * TX + cx - x0] = h.g3;
-                continue;
+        }
+        // ---- phase A: the halo edges, one kind per warp: x-edges at the three extra y-faces (warps 0-2), zU there
+        // (warps 3-5), y-edges at the three extra x-faces (warp 6) and zV there (warp 7)
+        if (warp < 3) {
+            const int row = warp == 0 ? 0 : TY + warp, b = y0 - 1 + row;
+            const EdgeTerms<T> h = x_edge(v4, w2, x, b, edge_coef(g, Y, b, ny), cze);
+            xw[row * TX + lane] = h.g1;
+            xw[G::NXW + row * TX + lane] = h.g3;
+        } else if (warp < 6) {
+            if (faces) {
+                const int row = warp == 3 ? 0 : TY + warp - 3, b = y0 - 1 + row;
+                const EdgeTerms<T> h = z_edge(u4[0], v4[0], x, b, cxo, edge_coef(g, Y, b, ny));
+                zu[row * TX + lane] = h.f1;
+                zu[G::NZU + row * TX + lane] = h.f3;
             }
-            r -= G::H_XE;
-            if (r < G::H_ZU) {                       // zU at y-faces y0-1, y0+TY, y0+TY+1
-                if (!faces) continue;
-                const int c = r / TX, cx = x0 + r % TX;
-                const int row = c == 0 ? 0 : TY + c;
-                const EdgeTerms<T> h = z_edge(cx, y0 - 1 + row, j, edge_coef(g, X, cx, nx), edge_coef(g, Y, y0 - 1 + row, ny));
-                S.zu1()[row * TX + cx - x0] = h.f1;
-                S.zu3()[row * TX + cx - x0] = h.f3;
-                continue;
+        } else if (lane < 3 * TY) {
+            const int c = lane / TY, col = c == 0 ? 0 : TX + c, ea = x0 - 1 + col, cy = y0 + lane % TY;
+            if (warp == 6) {
+                const EdgeTerms<T> h = y_edge(u4, w2, ea, cy, edge_coef(g, X, ea, nx), cze);
+                yw[(cy - y0) * EW + col] = h.g1;
+                yw[G::NYW + (cy - y0) * EW + col] = h.g3;
+            } else if (faces) {
+                const EdgeTerms<T> h = z_edge(u4[0], v4[0], ea, cy, edge_coef(g, X, ea, nx), edge_coef(g, Y, cy, ny));
+                zv[(cy - y0) * EW + col] = h.g1;
+                zv[G::NZV + (cy - y0) * EW + col] = h.g3;
             }
-            r -= G::H_ZU;
-            if (r < G::H_ZV) {                       // zV at x-faces x0-1, x0+TX, x0+TX+1
-                if (!faces) continue;
-                const int c = r / TY, cy = y0 + r % TY;
-                const int col = c == 0 ? 0 : TX + c;
-                const EdgeTerms<T> h = z_edge(x0 - 1 + col, cy, j, edge_coef(g, X, x0 - 1 + col, nx), edge_coef(g, Y, cy, ny));
-                S.zv1()[(cy - y0) * (TX + 3) + col] = h.g1;
-                S.zv3()[(cy - y0) * (TX + 3) + col] = h.g3;
-                continue;
-            }
-            r -= G::H_ZV;
-            if (j < z0 - 1) continue;                // K at the cells x0-1 (rows y0-1 ..) and y0-1 (x0 ..)
-            const int cx = r <= TY ? x0 - 1 : x0 + (r - TY - 1);
-            const int cy = r <= TY ? y0 - 1 + r : y0 - 1;
-            S.k(j)[(cy - y0 + 1) * KW + cx - x0 + 1] = k_cell(cx, cy, j);
         }
         __syncthreads();
 
-        // phase B: the faces of layer j
+        // ---- phase B: the faces of layer j
         if (faces && live) {
             const int z = j;
-            const T* kc = S.k(j) + (ty + 1) * KW + tx + 1;
-            const int om = (ty + 1) * MW + tx + 1;
-            const T* zu1 = S.zu1() + (ty + 1) * TX + tx;
-            const T* zu3 = S.zu3() + (ty + 1) * TX + tx;
-            const T* zv1 = S.zv1() + ty * (TX + 3) + tx + 1;
-            const T* zv3 = S.zv3() + ty * (TX + 3) + tx + 1;
+            const T* const kc = kj + (warp + 1) * KW + lane + 1;
+            const T* const km = base + G::OK + wrap(sk + 1, G::SK) * G::NK + (warp + 1) * KW + lane + 1;   // layer j-1
+            const int om = (warp + 1) * MW + lane + 1;
+            const T* const mprev[3] = {M(X, sm, 0), M(Y, sm, 0), M(Z, sm, 0)};      // layer (z-face) j-1
+            const T ispz0 = tab(g, Z, kInvSp, z), ispz1 = tab(g, Z, kInvSp, z + 1), iwz0 = tab(g, Z, kInvW, z);
             // viscous flux-form Laplacian of component A at (x, y, z) with wall and lid fluxes, then the RK
             // combination (the expressions of viscous_rk_tile, backend.cu:289-329)
-            auto finish = [&](auto Acomp, T L, T wall) {
+            auto visc = [&](auto Acomp, T L, T wall) {
                 constexpr int A = decltype(Acomp)::value;
-                const T* mc = S.m(A, z) + om;
+                const T* mc = mj[A] + om;
                 const T cc = mc[0];
-                const T mnb[3][2] = {{mc[-1], mc[1]}, {mc[-MW], mc[MW]}, {S.m(A, z - 1)[om], S.m(A, z + 1)[om]}};
-                const int q[3] = {x, y, z};
-                const int n[3] = {nx, ny, nz};
                 T lap = T(0);
-#pragma unroll
-                for (int t = 0; t < 3; t++) {
-                    const T lo_v = mnb[t][0], hi_v = mnb[t][1];
-                    if (t == A) {
-                        lap = lap + ((hi_v - cc) * tab(g, t, kInvW, q[t]) - (cc - lo_v) * tab(g, t, kInvW, q[t] - 1)) *
-                                        tab(g, t, kInvSp, q[t]);
-                        continue;
+                // x
+                if (A == X) {
+                    lap = lap + ((mc[1] - cc) * fx.iw0 - (cc - mc[-1]) * fx.iwm) * fx.is0;
+                } else {
+                    T hi = x < nx - 1 ? (mc[1] - cc) * fx.is1 : T(0);
+                    T lo = x > 0 ? (cc - mc[-1]) * fx.is0 : T(0);
+                    if (x == 0) lo = wall * fx.is0;
+                    if (x == nx - 1) hi = -wall * fx.is1;
+                    lap = lap + (hi - lo) * fx.iw0;
+                }
+                // y (the lid is the top wall)
+                if (A == Y) {
+                    lap = lap + ((mc[MW] - cc) * fy.iw0 - (cc - mc[-MW]) * fy.iwm) * fy.is0;
+                } else {
+                    T hi = y < ny - 1 ? (mc[MW] - cc) * fy.is1 : T(0);
+                    T lo = y > 0 ? (cc - mc[-MW]) * fy.is0 : T(0);
+                    if (y == 0) lo = wall * fy.is0;
+                    if (y == ny - 1) {
+                        const T Ul = A == X ? lidv * g.lid_u[x + (nx + 1) * z] : T(0);
+                        hi = (Ul - wall) * fy.is1;
                     }
-                    T hi = q[t] < n[t] - 1 ? (hi_v - cc) * tab(g, t, kInvSp, q[t] + 1) : T(0);
-                    T lo = q[t] > 0 ? (cc - lo_v) * tab(g, t, kInvSp, q[t]) : T(0);
-                    if (q[t] == 0) lo = wall * tab(g, t, kInvSp, 0);
-                    if (q[t] == n[t] - 1) {
-                        if (t == Y) {
-                            const T U = A == X ? lidv * g.lid_u[x + (nx + 1) * z] : T(0);
-                            hi = (U - wall) * tab(g, Y, kInvSp, n[Y]);
-                        } else {
-                            hi = -wall * tab(g, t, kInvSp, n[t]);
-                        }
-                    }
-                    lap = lap + (hi - lo) * tab(g, t, kInvW, q[t]);
+                    lap = lap + (hi - lo) * fy.iw0;
+                }
+                // z
+                const T zl = mprev[A][om], zh = mnext[A][om];
+                if (A == Z) {
+                    lap = lap + ((zh - cc) * iwz0 - (cc - zl) * tab(g, Z, kInvW, z - 1)) * ispz0;
+                } else {
+                    T hi = z < nz - 1 ? (zh - cc) * ispz1 : T(0);
+                    T lo = z > 0 ? (cc - zl) * ispz0 : T(0);
+                    if (z == 0) lo = wall * ispz0;
+                    if (z == nz - 1) hi = -wall * ispz1;
+                    lap = lap + (hi - lo) * iwz0;
                 }
                 const int i = fidx<A>(p, x, y, z);
-                T val = cc + dt * (a.nu * lap + L);
-                if (a.stage > 0) val = T(sc.a0) * a.m0[A][i] + T(sc.b) * val;
+                T val = cc + dt * (nu * lap + L);
+                if (a.stage > 0) val = a0 * a.m0[A][i] + b0 * val;
                 a.out[A][i] = val;
             };
             // u-face x
             {
                 const int i = fidx<X>(p, x, y, z);
-                if (blend) a.m0_out[X][i] = S.m(X, z)[om];
+                if (blend) a.m0_out[X][i] = mj[X][om];
                 if (x == 0) a.out[X][i] = T(0);
                 else {
-                    T L = half * (zu1[TX] + zu1[0]) + half * (yu1_1 + yu1_0);
+                    const T* z1p = zu + (warp + 1) * TX + lane;
+                    T L = half * (z1p[TX] + z1p[0]) + half * (yu1_1 + yu1_0);
                     if (o4) {
-                        const T c3 = tab(g, X, kC3, x);
-                        L = L + c3 * (zu3[2 * TX] + zu3[-TX]);
-                        L = L + c3 * (ye.f3 + yu3_m1);
+                        const T* z3p = z1p + G::NZU;
+                        L = L + fx.c3 * (z3p[2 * TX] + z3p[-TX]);
+                        L = L + fx.c3 * (ye.f3 + yu3_m1);
                     }
-                    L = L - (kc[0] - kc[-1]) * tab(g, X, kInvSp, x);
-                    finish(std::integral_constant<int, X>{}, L, S.u(z)[(ty + 3) * UW + tx + 1]);
+                    L = L - (kc[0] - kc[-1]) * fx.is0;
+                    visc(std::integral_constant<int, X>{}, L, u4[0][(warp + 3) * UW + lane + 1]);
                 }
                 if (x == nx - 1) {
-                    if (blend) a.m0_out[X][i + 1] = S.m(X, z)[om + 1];
+                    if (blend) a.m0_out[X][i + 1] = mj[X][om + 1];
                     a.out[X][i + 1] = T(0);
                 }
             }
             // v-face y
             {
                 const int i = fidx<Y>(p, x, y, z);
-                if (blend) a.m0_out[Y][i] = S.m(Y, z)[om];
+                if (blend) a.m0_out[Y][i] = mj[Y][om];
                 if (y == 0) a.out[Y][i] = T(0);
                 else {
-                    T L = half * (zv1[1] + zv1[0]) + half * (xv1_1 + xv1_0);
+                    const T* z1p = zv + warp * EW + lane + 1;
+                    T L = half * (z1p[1] + z1p[0]) + half * (xv1_1 + xv1_0);
                     if (o4) {
-                        const T c3 = tab(g, Y, kC3, y);
-                        L = L + c3 * (zv3[2] + zv3[-1]);
-                        L = L + c3 * (xe.f3 + xv3_m1);
+                        const T* z3p = z1p + G::NZV;
+                        L = L + fy.c3 * (z3p[2] + z3p[-1]);
+                        L = L + fy.c3 * (xe.f3 + xv3_m1);
                     }
-                    L = L - (kc[0] - kc[-KW]) * tab(g, Y, kInvSp, y);
-                    finish(std::integral_constant<int, Y>{}, L, S.v(z)[(ty + 1) * VW + tx + 3]);
+                    L = L - (kc[0] - kc[-KW]) * fy.is0;
+                    visc(std::integral_constant<int, Y>{}, L, v4[0][(warp + 1) * VW + lane + 3]);
                 }
                 if (y == ny - 1) {
-                    if (blend) a.m0_out[Y][i + nx] = S.m(Y, z)[om + MW];
+                    if (blend) a.m0_out[Y][i + nx] = mj[Y][om + MW];
                     a.out[Y][i + nx] = T(0);
                 }
             }
             // w-face z
             {
                 const int i = fidx<Z>(p, x, y, z);
-                if (blend) a.m0_out[Z][i] = S.m(Z, z)[om];
+                if (blend) a.m0_out[Z][i] = mj[Z][om];
                 if (z == 0) a.out[Z][i] = T(0);
                 else {
-                    const T* xw1 = S.xw(z) + (ty + 1) * TX + tx;
+                    const T* xw1 = base + G::OXW + se * 2 * G::NXW + (warp + 1) * TX + lane;     // plane j
                     const T* xw3 = xw1 + G::NXW;
-                    const T* yw1 = S.yw(z) + ty * (TX + 3) + tx + 1;
+                    const T* yw1 = base + G::OYW + se * 2 * G::NYW + warp * EW + lane + 1;
                     const T* yw3 = yw1 + G::NYW;
                     T L = half * (xw1[TX] + xw1[0]) + half * (yw1[1] + yw1[0]);
                     if (o4) {
@@ -444,11 +466,11 @@ __device__ void sweep_march_body(const MomentumArgs<T>& a, const Blk& blk) {
                         L = L + c3 * (xw3[2 * TX] + xw3[-TX]);
                         L = L + c3 * (yw3[2] + yw3[-1]);
                     }
-                    L = L - (kc[0] - S.k(z - 1)[(ty + 1) * KW + tx + 1]) * tab(g, Z, kInvSp, z);
-                    finish(std::integral_constant<int, Z>{}, L, S.w(z)[(ty + 3) * WW + tx + 3]);
+                    L = L - (kc[0] - km[0]) * ispz0;
+                    visc(std::integral_constant<int, Z>{}, L, w0[(warp + 3) * WW + lane + 3]);
                 }
                 if (z == nz - 1) {
-                    if (blend) a.m0_out[Z][i + nx * ny] = S.m(Z, z + 1)[om];
+                    if (blend) a.m0_out[Z][i + nx * ny] = mnext[Z][om];
                     a.out[Z][i + nx * ny] = T(0);
                 }
             }

@@ -1,5 +1,7 @@
 """The autotuner (cavity_autotune): it leaves the cavity's state as it was, picks one of its candidates, and the
-steps it then runs are bit-identical to an untuned cavity's; the choice is written to CAVITY_TUNE_FILE."""
+steps it then runs equal an untuned cavity's: bit for bit when the sweep kernel is fixed (CAVITY_SWEEP=tile: the
+other choices only change launch shapes), to rounding when the tuner may also pick the march sweep (1e-12 in
+FP64, 1e-6 in the FP32 fields of the mixed form); the choice is written to CAVITY_TUNE_FILE."""
 import numpy as np
 import pytest
 
@@ -10,10 +12,13 @@ pytestmark = pytest.mark.gpu
 FIELDS = ('u', 'v', 'w', 'mx', 'my', 'mz', 'phi')
 
 
+@pytest.mark.parametrize('sweep', ['tile', None])
 @pytest.mark.parametrize('precision', ['fp64', 'mixed'])
-def test_autotune_keeps_state_and_results(precision, tmp_path, monkeypatch):
+def test_autotune_keeps_state_and_results(precision, sweep, tmp_path, monkeypatch):
     tune_file = tmp_path / 'tune.txt'
     monkeypatch.setenv('CAVITY_TUNE_FILE', str(tune_file))
+    if sweep:
+        monkeypatch.setenv('CAVITY_SWEEP', sweep)
     s = workloads.settings(48, 1000.0, nz=40, beta=1.5, cfl=0.5)
     a, b = Cavity(s, precision=precision), Cavity(s, precision=precision)
     try:
@@ -30,11 +35,17 @@ def test_autotune_keeps_state_and_results(precision, tmp_path, monkeypatch):
         assert a.report() == rep
         for k in FIELDS:
             assert np.array_equal(a.field(k), before[k]), k
+        tol = 0.0 if sweep else (1e-12 if precision == 'fp64' else 1e-6)
         for _ in range(4):
             ra, rb = a.step(), b.step()
-            assert ra == rb
+            assert ra['steps'] == rb['steps'] and ra['phi_passes'] == rb['phi_passes']
+            assert abs(ra['time'] - rb['time']) <= tol * rb['time']
         for k in FIELDS:
-            assert np.array_equal(a.field(k), b.field(k)), k
+            x, y = a.field(k), b.field(k)
+            if sweep:
+                assert np.array_equal(x, y), k
+            else:
+                assert float(np.abs(x - y).max()) <= tol * max(float(np.abs(y).max()), 1e-30), k
     finally:
         a.close()
         b.close()
