@@ -188,6 +188,60 @@ def cell_kernel_bytes(settings, field_bytes):
             'finish': 2 * faces * field_bytes + 32 * cells}
 
 
+def gemm_peak_tflops(kind):
+    """Measured tensor-core GEMM rate of this GPU through cuBLAS (torch.matmul), the denominator of the transforms'
+    roofline: 'fp64' (DGEMM, 8192^3) or 'tf32' (FP32 GEMM with TF32 tensor cores, 16384^3); best of 5."""
+    import torch
+    n = 8192 if kind == 'fp64' else 16384
+    dtype = torch.float64 if kind == 'fp64' else torch.float32
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = kind == 'tf32'
+    try:
+        a = torch.randn(n, n, device='cuda', dtype=dtype)
+        b = torch.randn(n, n, device='cuda', dtype=dtype)
+        torch.matmul(a, b)
+        best = None
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
+def uses_tensor_cores(settings, precision):
+    """Whether the library runs a cavity's transforms on tcgen05 (the mixed form from 128^3 cells up, nx a multiple
+    of 4, unless CAVITY_FDM says otherwise): the rule of Solver's constructor."""
+    fdm = os.environ.get('CAVITY_FDM', '')
+    cells = settings['nx'] * settings['ny'] * settings['nz']
+    return precision == 'mixed' and settings['nx'] % 4 == 0 and (fdm == 'tc' or (fdm != 'dmma' and cells >= 1 << 21))
+
+
+def transforms_roofline(settings, ms_per_pass, tc, peak_gbs):
+    """The six transforms of a pressure pass: FLOP/s against the measured cuBLAS rate of their arithmetic (FP64
+    DMMA against DGEMM; the mixed form's 3xTF32 tensor-core products, counted three times, against TF32 GEMM), and
+    bytes against HBM: 16 B per cell per transform (an 8-byte read and write; the first reads the FP64
+    residual, the last updates the FP64 potential) plus 8 B of 1/lambda."""
+    nx, ny, nz = settings['nx'], settings['ny'], settings['nz']
+    cells = nx * ny * nz
+    flops = 4.0 * (nx + ny + nz) * cells * (3 if tc else 1)
+    nbytes = (6 * 16 + 8) * cells
+    s = ms_per_pass / 1e3
+    peak = gemm_peak_tflops('tf32' if tc else 'fp64')
+    return {'kernel': 'tc_transform_kernel (3xTF32)' if tc else 'dgemm_mma_kernel (FP64 DMMA)',
+            'ms_per_pass': ms_per_pass, 'flops_per_pass': flops, 'achieved_tflops': flops / s / 1e12,
+            'peak_tflops': peak, 'peak_kind': 'measured cuBLAS ' + ('TF32' if tc else 'DGEMM') + ' on this GPU',
+            'tensor_frac': flops / s / 1e12 / peak, 'bytes_per_pass': nbytes, 'achieved_gbs': nbytes / s / 1e9,
+            'hbm_frac': nbytes / s / 1e9 / peak_gbs}
+
+
 def cpu_oracle_rate(workload, steps_budget_s=12.0, max_steps=40, warmup=1):
     """The FP64 OpenMP oracle on this host: cell-updates/s over a bounded number of steps after `warmup`."""
     from les_impulse3d_64_b200 import workloads
@@ -370,6 +424,7 @@ def run_ours(args, ranks):
                      'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': profile_traffic(args.workload), 'ms_per_launch': kernel_s * 1e3},
         'stencil_kernels': cell_kernels,
+        'transforms': transforms_roofline(s, ranks.max(ktimes['transforms']) / 3, uses_tensor_cores(s, precision), peak),
         'clocks': clocks.summary(),
     }
     if not args.no_batched and args.workload == 'c2_64cube_re1000':

@@ -112,9 +112,9 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
  * tile (0: the size rule) and one-launch choice (1 yes, 0 no, -1 the size rule), and the step time in
  * milliseconds. */
 int cavity_autotune(CavitySolver* s, int steps, int* march_chunks, int* dgemm_tile, int* fused_pass, float* ms_per_step);
-/* After cavity_time_steps: ms[4] receives the mean device time per timed step (milliseconds, all three stages)
- * of the momentum sweeps, the projection starts, the residuals of their warm-start guesses, and the finishes.
- * No counterpart in the reference. */
+/* After cavity_time_steps: ms[5] receives the mean device time per timed step (milliseconds, all three stages)
+ * of the momentum sweeps, the projection starts, the residuals of their warm-start guesses, the finishes, and
+ * the six transforms of each stage's first pressure pass.  No counterpart in the reference. */
 int cavity_kernel_times(CavitySolver* s, double* ms);
 /* The generalised eigenbasis of one axis's pressure operator, K S = W S diag(lambda) with S^T W S = I, for the grid
  * that `config` describes along `axis` (0 x, 1 y, 2 z): lambda[n] (the constant mode set to 0) and the row-major

@@ -316,12 +316,13 @@ class Cavity:
 
     def kernel_times(self):
         """Mean device time per step (ms, three stages) of the sweeps, projection starts, residuals of their
-        guesses and finishes, over the last `time_steps` call."""
+        guesses, finishes and the transforms of each stage's first pressure pass, over the last `time_steps`
+        call."""
         self.lib.cavity_kernel_times.argtypes = [ct.c_void_p, ct.c_void_p]
         self.lib.cavity_kernel_times.restype = ct.c_int
-        ms = np.zeros(4, dtype=np.float64)
+        ms = np.zeros(5, dtype=np.float64)
         self._call('cavity_kernel_times', self.handle, pointer(ms))
-        return dict(zip(('sweep', 'projection_start', 'guess_residual', 'finish'), (float(v) for v in ms)))
+        return dict(zip(('sweep', 'projection_start', 'guess_residual', 'finish', 'transforms'), (float(v) for v in ms)))
 
     def step_outputs_async(self, count=1, statistics=False):
         """Queue `count` steps, each followed on the device by its probe values and, if `statistics`, by the

@@ -710,8 +710,8 @@ public:
         if (ms_out) *ms_out = best.ms;
     }
 
-    // per-step device time of the sweeps, the projection starts, the residuals of their guesses and the finishes
-    // (all three stages) in the last time_steps call
+    // per-step device time of the sweeps, the projection starts, the residuals of their guesses, the finishes and
+    // the transforms of the first pass (all three stages) in the last time_steps call
     void kernel_times(double* ms) const override {
         for (int k = 0; k < kNumTimed; k++) ms[k] = timed_ms_[k];
     }
@@ -1015,6 +1015,11 @@ private:
     }
     // one pressure pass (backend.cu:801-814) followed by the residual that decides on the next
     void launch_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
+        launch_transforms(st, phi, h, use_h);
+        launch_residual(st, phi, h, use_h);
+    }
+    // the six transforms of a pass (backend.cu:801-814)
+    void launch_transforms(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, int use_h) {
         if (tc_fdm_) launch_tc_pass(st, phi, h, use_h != 0);
         else {
             const int outer = g_dgemm_tile;              // a batch's choice wins over this cavity's own tuning
@@ -1022,7 +1027,6 @@ private:
             launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h != 0, tune_.fused);
             g_dgemm_tile = outer;
         }
-        launch_residual(st, phi, h, use_h);
     }
     void launch_tc_pass(cudaStream_t st, double* phi, cudaGraphConditionalHandle h, bool use_h) {
         launch_tc_fdm_pass(st, tcop_, res_, rhs_, phi, reinterpret_cast<float*>(t1_), reinterpret_cast<float*>(t2_),
@@ -1050,7 +1054,7 @@ private:
     // A pressure refinement loop inside a stream capture: one pass, then a conditional while-node whose body is
     // one pass.  `first_residual` launches the kernels that set the loop condition before them.
     template <class F>
-    void captured_loop(F first_residual, double* phi) {
+    void captured_loop(F first_residual, double* phi, cudaEvent_t t0 = nullptr, cudaEvent_t t1 = nullptr) {
         cudaStreamCaptureStatus status;
         cudaGraph_t g;
         const cudaGraphNode_t* deps;
@@ -1061,7 +1065,10 @@ private:
         first_residual(h);
         // the first pass outside the loop: most solves need exactly one, and its kernels skip themselves when the
         // start decided on none (the first transform clears the loop condition either way)
-        launch_pass(stream_, phi, h, 1);
+        if (t0) check(cudaEventRecordWithFlags(t0, stream_, cudaEventRecordExternal));
+        launch_transforms(stream_, phi, h, 1);
+        if (t1) check(cudaEventRecordWithFlags(t1, stream_, cudaEventRecordExternal));
+        launch_residual(stream_, phi, h, 1);
         check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.type = cudaGraphNodeTypeConditional;
@@ -1108,15 +1115,18 @@ private:
                 launch_start(stream_, M_[out], true, stage, S, cur, 0, 0, between);
                 if (timing) mark(kev(kTkGuessResidual, stage)[1]);
                 pull_control();
-                while (hc_.cond && !hc_.error) {
-                    launch_pass(stream_, phi, 0, 0);
+                for (int pass = 0; hc_.cond && !hc_.error; pass++) {
+                    if (timing && pass == 0) mark(kev(kTkTransforms, stage)[0]);
+                    launch_transforms(stream_, phi, 0, 0);
+                    if (timing && pass == 0) mark(kev(kTkTransforms, stage)[1]);
+                    launch_residual(stream_, phi, 0, 0);
                     pull_control();
                 }
             } else {
                 captured_loop([&](cudaGraphConditionalHandle h) {
                     launch_start(stream_, M_[out], true, stage, S, cur, h, 1, between);
                     if (timing) mark(kev(kTkGuessResidual, stage)[1]);
-                }, phi);
+                }, phi, timing ? kev(kTkTransforms, stage)[0] : nullptr, timing ? kev(kTkTransforms, stage)[1] : nullptr);
             }
             if (timing) mark(kev(kTkFinish, stage)[0]);
             launch_finish(stream_, M_[out], U_[out], PHI_[out], true, stage, stage == 2);
@@ -1254,7 +1264,7 @@ private:
     cudaGraph_t graph_[2] = {nullptr, nullptr}, tgraph_[2] = {nullptr, nullptr};
     cudaGraphExec_t exec_[2] = {nullptr, nullptr}, texec_[2] = {nullptr, nullptr};
     // events of the timing graph: [kernel][stage][begin, end]; per-step means of the last time_steps call
-    enum TimedKernel : int { kTkSweep = 0, kTkStart, kTkGuessResidual, kTkFinish, kNumTimed };
+    enum TimedKernel : int { kTkSweep = 0, kTkStart, kTkGuessResidual, kTkFinish, kTkTransforms, kNumTimed };
     cudaEvent_t kev_[2 * 3 * kNumTimed] = {};
     cudaEvent_t* kev(int kind, int stage) { return kev_ + 2 * (3 * kind + stage); }
     double timed_ms_[kNumTimed] = {};

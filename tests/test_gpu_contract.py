@@ -184,8 +184,29 @@ def test_c2_mixed_matches_fp64_oracle(c2_oracle, c2_reference_errors, fdm, monke
         assert e['max_div'] <= 4 * e['max_div_oracle_float32'], (n, e)
 
 
+@pytest.fixture(scope='module')
+def c3_reference_errors():
+    """The reference's own backend.cu (FP32 fields) through C3's protocol against the FP64 oracle's fixture: the
+    error that FP32 fields carry at this config.  None where that build is absent."""
+    if not REFERENCE_BINARY.is_file():
+        return None
+    ref = np.load(GOLDEN / 'c3_oracle_1000.npz')
+    w = workloads.C3
+    steps = int(ref['steps'])
+    rr, sr, _, _ = play(lambda s: Solver(s, library=REFERENCE_BINARY), w, snapshots=(steps,), steps=steps)
+    f, diag = sr[steps]
+    e = mixed_errors(f, diag, {k: ref[f'layer.{k}'] for k in ('u', 'v', 'w', 'phi')},
+                     {'kinetic_energy': float(ref['diag.kinetic_energy'])}, w['settings'],
+                     layers=[int(k) for k in ref['layers']])
+    e['dt_reason_same'] = bool(list(rr['dt_reason']) == [str(x) for x in ref['run.dt_reason']])
+    e['norm_rel'] = {k: abs(float(np.linalg.norm(f[k])) - float(ref[f'norm.{k}'])) / float(ref[f'norm.{k}'])
+                     for k in ('u', 'v', 'w', 'phi')}
+    _record('c3_reference_backend_fp32_vs_oracle', e)
+    return {steps: e}
+
+
 @pytest.mark.parametrize('fdm', ['default', 'dmma'])
-def test_c3_mixed_matches_fp64_oracle_fixture(fdm, monkeypatch):
+def test_c3_mixed_matches_fp64_oracle_fixture(fdm, monkeypatch, c3_reference_errors):
     """C3, 1000 steps of the mixed form (tensor-core transforms by default at 128^3, or the FP64 DMMA ones)
     against the FP64 oracle's run of the same seeded workload (tests/golden/c3_oracle_1000.npz): errors on
     the fixture's z-layers, kinetic energy and full-field norms, and the max |div u| of the whole field."""
@@ -212,9 +233,11 @@ def test_c3_mixed_matches_fp64_oracle_fixture(fdm, monkeypatch):
     e['passes_per_stage'] = float(rg['phi_passes'].mean())
     _record(f'c3_mixed_{fdm}_vs_oracle', e)
     assert e['dt_reason_same']
-    assert e['velocity_rel_l2'] <= 1e-5, e
-    assert e['kinetic_energy_rel'] <= 1e-5, e
-    assert e['phi_rel_l2'] <= 1e-4, e
-    assert max(e['norm_rel'].values()) <= 1e-5, e
+    ref_e = c3_reference_errors
+    assert e['velocity_rel_l2'] <= mixed_bound('velocity_rel_l2', steps, ref_e, 1e-5), e
+    assert e['kinetic_energy_rel'] <= mixed_bound('kinetic_energy_rel', steps, ref_e, 1e-5), e
+    assert e['phi_rel_l2'] <= mixed_bound('phi_rel_l2', steps, ref_e, 1e-4), e
+    for k, r in e['norm_rel'].items():
+        assert r <= (1e-5 if ref_e is None else max(1e-5, 2.0 * ref_e[steps]['norm_rel'][k])), (k, e)
     assert e['div_rms'] < 1e-5, e
     assert e['max_div'] <= 4 * e['max_div_oracle_float32'], e
