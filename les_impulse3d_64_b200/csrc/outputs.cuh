@@ -174,6 +174,22 @@ __global__ void probes_kernel(OutArgs<T> a, const int* cells, int n, float* out)
     out[2 * k + 1] = (float)centred(a, 1, x, y, z);
 }
 
+// After a step (single cavities): the probe values and the control block into pinned, mapped host memory, so that
+// the blocking per-step calls of the reference's front end (solver_step's report, solver_probes) read host memory
+// after the step's one wait instead of each queueing a copy and waiting again.
+template <class T>
+__global__ void step_tail_kernel(OutArgs<T> a, const int* cells, int n, float* probes, const Control* c, Control* c_host) {
+    const int k = threadIdx.x;
+    if (k < n) {
+        const int x = cells[3 * k], y = cells[3 * k + 1], z = cells[3 * k + 2];
+        probes[2 * k] = (float)centred(a, 0, x, y, z);
+        probes[2 * k + 1] = (float)centred(a, 1, x, y, z);
+    }
+    const int* src = reinterpret_cast<const int*>(c);
+    int* dst = reinterpret_cast<int*>(c_host);
+    for (int i = k; i < (int)(sizeof(Control) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+}
+
 // mid-span layers: the plane z = LZ/2 lies between k1 and k2 (backend.cu:488)
 __device__ __forceinline__ void midspan_layers(int nz, int& k1, int& k2) { k2 = nz / 2; k1 = (nz % 2) ? k2 : k2 - 1; }
 

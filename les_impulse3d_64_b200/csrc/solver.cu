@@ -245,12 +245,14 @@ public:
         arena_.release();
         if (flush_) cudaFree(flush_);
         if (ring_host_) cudaFreeHost(ring_host_);
+        if (tail_host_) cudaFreeHost(tail_host_);
         if (stream_) cudaStreamDestroy(stream_);
         if (body_stream_) cudaStreamDestroy(body_stream_);
     }
 
     // -------------------------------------------------------------------------------- ABI operations
     void initialize(const double* v_noise, const double* w_noise) override {         // backend.cu:1075-1088
+        probes_fresh_ = false;
         const double* src[3] = {nullptr, v_noise, w_noise};
         for (int k = 0; k < 3; k++) {
             if (src[k]) check(cudaMemcpyAsync(dstage_[0], src[k], sizeof(double) * size_[k], cudaMemcpyHostToDevice, stream_));
@@ -268,17 +270,32 @@ public:
         if (auto_tune_ && tune_.ms == 0 && pending_.empty()) autotune(6, nullptr, nullptr, nullptr, nullptr);
         ensure_graphs(false);
         if (pending_.empty()) steps_before_ = hc_.steps;
+        if (!tail_host_) {
+            const size_t off = 256 * ((sizeof(Control) + 255) / 256);
+            check(cudaHostAlloc(&tail_host_, off + sizeof(float) * 16, cudaHostAllocMapped));
+            check(cudaHostGetDevicePointer(&tail_dev_, tail_host_, 0));
+        }
+        probes_fresh_ = false;
         for (int i = 0; i < count; i++) {
             if (eager_) enqueue_step(par_, false, true);
             else check(cudaGraphLaunch(exec_[par_], stream_));
             // the parity flips only when the step succeeds; sync() checks that for the queued steps
             pending_.push_back(par_);
             par_ ^= 1;
+            char* d = static_cast<char*>(tail_dev_);
+            step_tail_kernel<T><<<1, 32, 0, stream_>>>(out_args(), probe_cells_, c_.n_probes,
+                                                       reinterpret_cast<float*>(d + 256 * ((sizeof(Control) + 255) / 256)),
+                                                       ctrl_, reinterpret_cast<Control*>(d));
         }
+        tail_queued_ = true;
     }
     void sync(CavityReport* r) override {
         check(cudaStreamSynchronize(stream_));
-        pull_control();
+        if (tail_queued_) std::memcpy(&hc_, tail_control(), sizeof hc_);      // written by the last step's tail
+        else pull_control();
+        const bool tail = tail_queued_;
+        tail_queued_ = false;
+        probes_fresh_ = false;
         const size_t queued = pending_.size();
         const std::vector<int> pending_copy = pending_;
         pending_.clear();
@@ -294,6 +311,7 @@ public:
             raise_error(code);
         }
         check(cudaGetLastError());
+        probes_fresh_ = tail && !pending_copy.empty();
         if (r) report(r);
     }
     void report(CavityReport* r) override {
@@ -302,6 +320,7 @@ public:
     }
 
     void kick(const double* const noise[3], double amp, int passes) override {        // backend.cu:958-978
+        probes_fresh_ = false;
         const int S = par_, X2 = par_ ^ 1;
         for (int k = 0; k < 3; k++) {
             const int sx = nx_ + (k == 0), sy = ny_ + (k == 1), sz = nz_ + (k == 2);
@@ -388,6 +407,7 @@ public:
         check(cudaStreamSynchronize(stream_));
     }
     void set_field(int field, const void* in) override {                              // backend.cu:1147-1155
+        probes_fresh_ = false;
         if (field < 0 || field > 6) fail("field must be 0..6");
         if (field == 6) {
             check(cudaMemcpyAsync(PHI_[par_], in, sizeof(double) * n_cell_, cudaMemcpyHostToDevice, stream_));
@@ -503,6 +523,7 @@ public:
         check(cudaStreamSynchronize(stream_));
     }
     void checkpoint_load(const void* src, int device) override {
+        probes_fresh_ = false;
         if (!pending_.empty()) fail("checkpoint: steps are queued; sync first");
         const CkLayout L = ck_layout();
         const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -535,6 +556,10 @@ public:
     }
     void probes(float* out) override {                                                // backend.cu:1159-1166
         if (c_.n_probes == 0) return;
+        if (probes_fresh_) {           // the last step's tail computed them from the current state
+            std::memcpy(out, tail_probes(), sizeof(float) * 2 * c_.n_probes);
+            return;
+        }
         probes_kernel<T><<<1, 32, 0, stream_>>>(out_args(), probe_cells_, c_.n_probes, probe_out_);
         check(cudaMemcpyAsync(out, probe_out_, sizeof(float) * 2 * c_.n_probes, cudaMemcpyDeviceToHost, stream_));
         check(cudaStreamSynchronize(stream_));
@@ -577,6 +602,7 @@ public:
     // given, `steps` more through the graph with events around the kernels (they cost launch latency, so the step
     // times come from the plain graph), for the per-kernel times
     void time_steps(int warmup, int steps, int flush, float* ms, float* kms) override {
+        probes_fresh_ = false;
         if (flush && !flush_) check(cudaMalloc(&flush_, kFlushBytes));
         for (int i = 0; i < warmup; i++) step(nullptr);      // (the first may run the autotuner, which rebuilds graphs)
         ensure_graphs(false);
@@ -1269,6 +1295,14 @@ private:
     cudaEvent_t* kev(int kind, int stage) { return kev_ + 2 * (3 * kind + stage); }
     double timed_ms_[kNumTimed] = {};
     void* flush_ = nullptr;
+    // the step tail's outputs (step_tail_kernel): one pinned, mapped block holding the control block and the probe
+    // values after the last step queued through step_async
+    void* tail_host_ = nullptr;
+    void* tail_dev_ = nullptr;
+    bool tail_queued_ = false;          // the last queued step has its tail
+    bool probes_fresh_ = false;         // the tail's probe values are those of the current state
+    Control* tail_control() const { return static_cast<Control*>(tail_host_); }
+    float* tail_probes() const { return reinterpret_cast<float*>(static_cast<char*>(tail_host_) + 256 * ((sizeof(Control) + 255) / 256)); }
     float* ring_host_ = nullptr;       // queued per-step probe values (pinned, mapped)
     float* ring_dev_ = nullptr;
     int ring_n_ = 0;
@@ -1361,6 +1395,8 @@ public:
                 if (s->pending_.empty()) s->steps_before_ = s->hc_.steps;
                 s->pending_.push_back(s->par_);
                 s->par_ ^= 1;
+                s->tail_queued_ = false;          // a batch step has no per-cavity tail: sync reads the control block
+                s->probes_fresh_ = false;
             }
             par_ ^= 1;
             queued_ = true;
