@@ -234,7 +234,12 @@ inline void launch_transform(cudaStream_t st, int M, int N, int K, const double*
     const GemmArgs<double> g = transform_args(M, N, K, A, A_alt, lda, sA, B, ldb, sB, C, ldc, sC, epi, inv_lambda, phi,
                                               c, h, clear);
     const long long tiles64 = (long long)((N + 63) / 64) * ((M + 63) / 64) * batch * g_launch_batch;
-    if (g_dgemm_tile ? g_dgemm_tile == 64 : tiles64 >= 296) {
+    static const int forced = [] {                 // CAVITY_DGEMM_TILE=32 or 64 forces the tile everywhere
+        const char* e = std::getenv("CAVITY_DGEMM_TILE");
+        return e ? std::atoi(e) : 0;
+    }();
+    const int tile = forced ? forced : g_dgemm_tile;
+    if (tile ? tile == 64 : tiles64 >= 296) {
         dim3 grid((N + 63) / 64, (M + 63) / 64, batch);
         if (!record_launch(kLkDgemm64, 0, grid, 0, g)) launch_pdl(dgemm_mma_kernel<64, 64, 2, 2, 32>, grid, dim3(128), 0, st, g);
     } else {
