@@ -69,12 +69,19 @@ def c2_oracle(oracle_libs):
 REFERENCE_BINARY = Path(__file__).resolve().parents[1] / 'oracle' / '_ref' / 'libcavity_solver.so'
 
 
+def recorded_reference_errors(config):
+    """The reference build's errors recorded on a B200, keyed by step number."""
+    rec = json.loads((GOLDEN / 'reference_fp32_errors.json').read_text())[config]
+    return {int(n): e for n, e in rec.items()}
+
+
 @pytest.fixture(scope='module')
 def c2_reference_errors(c2_oracle):
     """The reference's own backend.cu (FP32 fields, built unchanged under oracle/_ref) through C2's protocol,
-    against the FP64 oracle: the error that FP32 fields carry at this config.  None where that build is absent."""
+    against the FP64 oracle: the error that FP32 fields carry at this config.  Where that build is absent, the
+    errors it gave on a B200 (tests/golden/reference_fp32_errors.json)."""
     if not REFERENCE_BINARY.is_file():
-        return None
+        return recorded_reference_errors('c2')
     w = workloads.C2
     ro, so, _, _ = c2_oracle
     rr, sr, _, _ = play(lambda s: Solver(s, library=REFERENCE_BINARY), w)
@@ -187,9 +194,9 @@ def test_c2_mixed_matches_fp64_oracle(c2_oracle, c2_reference_errors, fdm, monke
 @pytest.fixture(scope='module')
 def c3_reference_errors():
     """The reference's own backend.cu (FP32 fields) through C3's protocol against the FP64 oracle's fixture: the
-    error that FP32 fields carry at this config.  None where that build is absent."""
+    error that FP32 fields carry at this config.  Where that build is absent, the errors it gave on a B200."""
     if not REFERENCE_BINARY.is_file():
-        return None
+        return recorded_reference_errors('c3')
     ref = np.load(GOLDEN / 'c3_oracle_1000.npz')
     w = workloads.C3
     steps = int(ref['steps'])
