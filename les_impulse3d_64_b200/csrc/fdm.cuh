@@ -155,6 +155,347 @@ __global__ void __launch_bounds__(WARPS_M * WARPS_N * 32) dgemm_mma_batched(cons
     dgemm_mma_body<BM, BN, WARPS_M, WARPS_N, KC>(g, k, first_block());
 }
 
+// ---------------------------------------------------------------------------------------------- paired pass
+// The six transforms of a pass as three launches when no axis has more than 64 cells.  Each launch chains two
+// transforms through shared memory, so the intermediate between them never goes back to memory:
+//   pair_xy_kernel:  t = ST_y (r S_x)                      a CTA per z-plane and block of W x-columns
+//   pair_z_kernel:   t = S_z (inv_lambda .* (ST_z t))      a CTA per block of W plane columns, in place
+//   pair_yx_kernel:  phi += (S_y t) ST_x                   a CTA per z-plane and block of W y-rows
+// Every dot product runs over k in the same order, four at a time from a zero accumulator, as in
+// dgemm_mma_body, and the values between the transforms are the same doubles, so each transform's result is
+// bit for bit the six-launch pass's.  Shared-memory operands are zero outside the matrices up to the next
+// multiple of 8 (rows) or 4 (k), as the six-launch pass's staged panels are.
+constexpr int kPairMax = 64;                 // the largest axis a paired pass takes
+constexpr int kPairPitch = kPairMax + 4;     // row pitch of a 64-wide operand: 8 banks mod 32
+constexpr int kPairThreads = 256;
+
+struct FdmPairArgs {
+    int nx, ny, nz, clear_condition;
+    const double* s[3];
+    const double* st[3];
+    const double* inv_lambda;
+    const double* r;
+    const double* r_alt;            // used instead of r when the control block says use_rhs
+    double* t;                      // nx*ny*nz doubles of scratch
+    double* phi;
+    const Control* c;
+    cudaGraphConditionalHandle handle;
+};
+
+__device__ __forceinline__ int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// dst[i * p + k] = src[i * ld + k] for i < rows, k < cols, and 0 elsewhere in the R x C extent (C even), as
+// cp.async copies of two doubles where alignment allows, else of one
+__device__ __forceinline__ void pair_stage(double* dst, int p, const double* src, long long ld, int rows, int cols,
+                                           int R, int C) {
+    const bool two = ld % 2 == 0 && ((unsigned long long)src & 15) == 0;
+    if (two) {
+        for (int e = threadIdx.x; e < R * C / 2; e += kPairThreads) {
+            const int i = e / (C / 2), k = 2 * (e % (C / 2));
+            const int n = i < rows ? min(2, max(0, cols - k)) : 0;
+            cp_async16z(&dst[i * p + k], n ? src + i * ld + k : src, 8 * n);
+        }
+    } else {
+        for (int e = threadIdx.x; e < R * C; e += kPairThreads) {
+            const int i = e / C, k = e % C;
+            const bool ok = i < rows && k < cols;
+            cp_async8(&dst[i * p + k], ok ? src + i * ld + k : src, ok ? 8 : 0);
+        }
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// acc += A[m0 .., 0 .. k4) B[0 .. k4, n0 ..) for one warp's FM x FN fragments of 8 x 8 (k4 a multiple of 4)
+template <int FM, int FN>
+__device__ __forceinline__ void pair_warp_mma(double (&acc)[FM][FN][2], const double* As, int lda, const double* Bs,
+                                              int ldb, int k4, int m0, int n0) {
+    const int lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+#pragma unroll
+    for (int i = 0; i < FM; i++)
+#pragma unroll
+        for (int j = 0; j < FN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int kk = 0; kk < k4; kk += 4) {
+        double af[FM], bf[FN];
+#pragma unroll
+        for (int i = 0; i < FM; i++) af[i] = As[(m0 + i * 8 + fr) * lda + kk + fc];
+#pragma unroll
+        for (int j = 0; j < FN; j++) bf[j] = Bs[(kk + fc) * ldb + n0 + j * 8 + fr];
+#pragma unroll
+        for (int i = 0; i < FM; i++)
+#pragma unroll
+            for (int j = 0; j < FN; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+}
+
+// The pass's entry checks (as dgemm_mma_body's): programmatic launch, the loop guard, error and residual.
+// False when the block has nothing to do.
+__device__ __forceinline__ bool pair_enter(const FdmPairArgs& a, bool first, bool clear) {
+    pdl_launch_dependents();
+    pdl_wait();
+    if (clear && a.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(a.handle, 0u);
+    const Control* c = a.c;
+    if (c->error || !c->cond) return false;
+    const double r2 = c->use_rhs ? c->rhs_norm2 : c->res_norm2;
+    return r2 > 0;
+}
+
+template <int W> struct PairSmem {
+    // two square operands of pitch kPairPitch and two 64 x W panels of pitch W + 4
+    static constexpr int kPanel = W + 4;
+    static constexpr size_t bytes = sizeof(double) * (2 * kPairMax * kPairPitch + 2 * kPairMax * kPanel);
+};
+
+// t[z] = ST_y (r[z] S_x) on columns [x0, x0 + W) of plane z: transforms 1 and 2 of the pass
+template <int W>
+__device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
+    if (!pair_enter(a, first, true)) return;
+    constexpr int PW = PairSmem<W>::kPanel, FN = W / 8;
+    extern __shared__ __align__(16) double pair_smem[];
+    double* A1 = pair_smem;                         // r[z]: ny x nx
+    double* A2 = A1 + kPairMax * kPairPitch;        // ST_y: ny x ny
+    double* B1 = A2 + kPairMax * kPairPitch;        // S_x[:, x0 .. x0 + W)
+    double* C1 = B1 + kPairMax * PW;                // r[z] S_x on those columns
+    const int nx = a.nx, ny = a.ny, z = blk.y, x0 = blk.x * W;
+    const double* r = (a.r_alt && a.c->use_rhs ? a.r_alt : a.r) + (long long)z * nx * ny;
+    const int my = round_up(ny, 8), kx = round_up(nx, 4), ky = round_up(ny, 4);
+    pair_stage(A1, kPairPitch, r, nx, ny, nx, my, round_up(kx, 2));
+    pair_stage(B1, PW, a.s[X] + x0, nx, nx, min(W, nx - x0), kx, W);
+    cp_async_commit();
+    pair_stage(A2, kPairPitch, a.st[Y], ny, ny, ny, my, round_up(ky, 2));
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+    const int m0 = warp * 8;                        // the warp's 8 rows (y) x W columns
+    double acc[1][FN][2];
+    if (m0 < my) {
+        pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, PW, kx, m0, 0);
+#pragma unroll
+        for (int j = 0; j < FN; j++) {
+            C1[(m0 + fr) * PW + j * 8 + 2 * fc] = acc[0][j][0];
+            C1[(m0 + fr) * PW + j * 8 + 2 * fc + 1] = acc[0][j][1];
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (m0 >= my) return;
+    pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, ky, m0, 0);
+    const int y = m0 + fr;
+    if (y >= ny) return;
+    double* t = a.t + ((long long)z * ny + y) * nx;
+#pragma unroll
+    for (int j = 0; j < FN; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int x = x0 + j * 8 + 2 * fc + h;
+            if (x < nx) t[x] = acc[0][j][h];
+        }
+}
+
+// t[:, c] = S_z (inv_lambda .* (ST_z t[:, c])) on plane columns c in [c0, c0 + W), in place: transforms 3 and 4
+template <int W>
+__device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
+    if (!pair_enter(a, first, false)) return;
+    constexpr int PW = PairSmem<W>::kPanel, FN = W / 8;
+    extern __shared__ __align__(16) double pair_smem[];
+    double* A1 = pair_smem;                         // ST_z
+    double* A2 = A1 + kPairMax * kPairPitch;        // S_z
+    double* B1 = A2 + kPairMax * kPairPitch;        // t[:, c0 .. c0 + W)
+    double* C1 = B1 + kPairMax * PW;
+    const int nz = a.nz, plane = a.nx * a.ny, c0 = blk.x * W;
+    const int mz = round_up(nz, 8), kz = round_up(nz, 4);
+    pair_stage(A1, kPairPitch, a.st[Z], nz, nz, nz, mz, round_up(kz, 2));
+    pair_stage(B1, PW, a.t + c0, plane, nz, min(W, plane - c0), kz, W);
+    cp_async_commit();
+    pair_stage(A2, kPairPitch, a.s[Z], nz, nz, nz, mz, round_up(kz, 2));
+    cp_async_commit();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+    const int m0 = warp * 8;
+    double acc[1][FN][2], il[FN][2];
+    if (m0 < mz) {
+        const int z = m0 + fr;
+#pragma unroll
+        for (int j = 0; j < FN; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int c = c0 + j * 8 + 2 * fc + h;
+                il[j][h] = z < nz && c < plane ? __ldg(a.inv_lambda + (long long)z * plane + c) : 0.0;
+            }
+    }
+    cp_async_wait<1>();
+    __syncthreads();
+    if (m0 < mz) {
+        pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, PW, kz, m0, 0);
+#pragma unroll
+        for (int j = 0; j < FN; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) C1[(m0 + fr) * PW + j * 8 + 2 * fc + h] = acc[0][j][h] * il[j][h];
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (m0 >= mz) return;
+    pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, kz, m0, 0);
+    const int z = m0 + fr;
+    if (z >= nz) return;
+    double* t = a.t + (long long)z * plane;
+#pragma unroll
+    for (int j = 0; j < FN; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int c = c0 + j * 8 + 2 * fc + h;
+            if (c < plane) t[c] = acc[0][j][h];
+        }
+}
+
+// phi[z] += (S_y t[z]) ST_x on rows [y0, y0 + W) of plane z: transforms 5 and 6
+template <int W>
+__device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
+    if (!pair_enter(a, first, false)) return;
+    constexpr int WN = 8 / (W / 8), FN = kPairMax / 8 / WN;   // warps along x, fragments per warp along x
+    extern __shared__ __align__(16) double pair_smem[];
+    double* B1 = pair_smem;                         // t[z]: ny x nx
+    double* B2 = B1 + kPairMax * kPairPitch;        // ST_x: nx x nx
+    double* A1 = B2 + kPairMax * kPairPitch;        // S_y[y0 .. y0 + W, :]
+    double* C1 = A1 + W * kPairPitch;               // S_y t[z] on those rows
+    const int nx = a.nx, ny = a.ny, z = blk.y, y0 = blk.x * W;
+    const int kx = round_up(nx, 4), ky = round_up(ny, 4), mx = round_up(nx, 8);
+    const int cx = min(kPairMax, round_up(mx, 8 * FN));      // columns the active warps read: staged, zero past nx
+    pair_stage(A1, kPairPitch, a.s[Y] + (long long)y0 * ny, ny, min(W, ny - y0), ny, W, round_up(ky, 2));
+    pair_stage(B1, kPairPitch, a.t + (long long)z * nx * ny, nx, ny, nx, ky, cx);
+    cp_async_commit();
+    pair_stage(B2, kPairPitch, a.st[X], nx, nx, nx, kx, cx);
+    cp_async_commit();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
+    const int m0 = (warp / WN) * 8, n0 = (warp % WN) * FN * 8;    // the warp's 8 rows (y) x 8 FN columns (x)
+    const bool active = n0 < mx;
+    const int y = y0 + m0 + fr;
+    const int reset = a.c->reset_phi;
+    double* phi = a.phi + ((long long)z * ny + min(y, ny - 1)) * nx;
+    double old[FN][2];                              // the potential this thread updates, loaded ahead
+#pragma unroll
+    for (int j = 0; j < FN; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int x = n0 + j * 8 + 2 * fc + h;
+            old[j][h] = active && y < ny && x < nx && !reset ? phi[x] : 0.0;
+        }
+    cp_async_wait<1>();
+    __syncthreads();
+    double acc[1][FN][2];
+    if (active) {
+        pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, kPairPitch, ky, m0, n0);
+#pragma unroll
+        for (int j = 0; j < FN; j++) {
+            C1[(m0 + fr) * kPairPitch + n0 + j * 8 + 2 * fc] = acc[0][j][0];
+            C1[(m0 + fr) * kPairPitch + n0 + j * 8 + 2 * fc + 1] = acc[0][j][1];
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    if (!active) return;
+    pair_warp_mma<1, FN>(acc, C1, kPairPitch, B2, kPairPitch, kx, m0, n0);
+    if (y >= ny) return;
+#pragma unroll
+    for (int j = 0; j < FN; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int x = n0 + j * 8 + 2 * fc + h;
+            if (x < nx) phi[x] = old[j][h] + acc[0][j][h];
+        }
+}
+template <int W> struct PairYxSmem {
+    static constexpr size_t bytes = sizeof(double) * (2 * kPairMax * kPairPitch + 2 * W * kPairPitch);
+};
+
+constexpr int kPairW = 32;                   // columns (x, plane) or rows (y) of a paired-pass CTA
+enum PairPhase : int { kPairXy = 0, kPairZ = 1, kPairYx = 2 };
+
+__global__ void __launch_bounds__(kPairThreads, 2) pair_xy_kernel(FdmPairArgs a) {
+    pair_xy_body<kPairW>(a, real_blk(), first_block());
+}
+__global__ void __launch_bounds__(kPairThreads, 2) pair_z_kernel(FdmPairArgs a) {
+    pair_z_body<kPairW>(a, real_blk(), first_block());
+}
+__global__ void __launch_bounds__(kPairThreads, 2) pair_yx_kernel(FdmPairArgs a) {
+    pair_yx_body<kPairW>(a, real_blk(), first_block());
+}
+// a batch of cavities: grid x runs over the work list (BatchItem); the phase selects the body
+template <int PHASE>
+__global__ void __launch_bounds__(kPairThreads, 2) pair_batched(const FdmPairArgs* args, const BatchItem* items,
+                                                               const int* live) {
+    __shared__ FdmPairArgs a;
+    int cav;
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) {
+        if (PHASE == kPairXy) dead_slot_clear(args, items);
+        return;
+    }
+    load_args(a, args + cav);
+    if (PHASE == kPairXy) pair_xy_body<kPairW>(a, k, first_block());
+    else if (PHASE == kPairZ) pair_z_body<kPairW>(a, k, first_block());
+    else pair_yx_body<kPairW>(a, k, first_block());
+}
+inline size_t pair_smem_bytes(int phase) {
+    return phase == kPairYx ? PairYxSmem<kPairW>::bytes : PairSmem<kPairW>::bytes;
+}
+// grid of one phase for an nx x ny x nz cavity
+inline dim3 pair_grid(int phase, int nx, int ny, int nz) {
+    if (phase == kPairXy) return dim3((nx + kPairW - 1) / kPairW, nz);
+    if (phase == kPairZ) return dim3((nx * ny + kPairW - 1) / kPairW);
+    return dim3((ny + kPairW - 1) / kPairW, nz);
+}
+inline bool pair_pass_fits(int nx, int ny, int nz) {
+    return nx <= kPairMax && ny <= kPairMax && nz <= kPairMax;
+}
+// once per process, before any capture: the dynamic shared memory of the paired kernels
+inline cudaError_t pair_prepare() {
+    static const cudaError_t e = [] {
+        cudaError_t r = cudaFuncSetAttribute(pair_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)pair_smem_bytes(kPairXy));
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(pair_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem_bytes(kPairZ));
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(pair_yx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem_bytes(kPairYx));
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(pair_batched<kPairXy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pair_smem_bytes(kPairXy));
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(pair_batched<kPairZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pair_smem_bytes(kPairZ));
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(pair_batched<kPairYx>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pair_smem_bytes(kPairYx));
+        return r;
+    }();
+    return e;
+}
+inline void launch_fdm_pass_pairs(cudaStream_t st, const FdmOperands& op, const double* r, const double* r_alt,
+                                  double* phi, double* t, const Control* c, cudaGraphConditionalHandle h, bool clear) {
+    FdmPairArgs a;
+    a.nx = op.nx; a.ny = op.ny; a.nz = op.nz;
+    a.clear_condition = clear;
+    for (int k = 0; k < 3; k++) { a.s[k] = op.s[k]; a.st[k] = op.st[k]; }
+    a.inv_lambda = op.inv_lambda;
+    a.r = r; a.r_alt = r_alt; a.t = t; a.phi = phi; a.c = c; a.handle = h;
+    void (*kernels[3])(FdmPairArgs) = {pair_xy_kernel, pair_z_kernel, pair_yx_kernel};
+    for (int ph = 0; ph < 3; ph++) {
+        const dim3 grid = pair_grid(ph, op.nx, op.ny, op.nz);
+        if (!record_launch(kLkPair, ph, grid, pair_smem_bytes(ph), a))
+            launch_pdl(kernels[ph], grid, dim3(kPairThreads), pair_smem_bytes(ph), st, a);
+    }
+}
+// a recorded paired launch (variant: the phase) over a batch of cavities
+inline void launch_pair_batched(int phase, dim3 grid, const BatchItem* items, const int* live, const FdmPairArgs* d,
+                                cudaStream_t st) {
+    const size_t smem = pair_smem_bytes(phase);
+    if (phase == kPairXy) launch_pdl(pair_batched<kPairXy>, grid, dim3(kPairThreads), smem, st, d, items, live);
+    else if (phase == kPairZ) launch_pdl(pair_batched<kPairZ>, grid, dim3(kPairThreads), smem, st, d, items, live);
+    else launch_pdl(pair_batched<kPairYx>, grid, dim3(kPairThreads), smem, st, d, items, live);
+}
+
 // ---------------------------------------------------------------------------------------------- one-launch pass
 // The six transforms of a pass as phases of one cooperative launch, separated by grid barriers: a small grid's
 // transforms are each a few microseconds of latency-bound work, and one launch replaces six.  Each phase runs
@@ -301,21 +642,38 @@ inline void launch_fdm_pass_fused(cudaStream_t st, const FdmOperands& op, const 
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, fdm_pass_fused_kernel, a);
 }
-// the one-launch pass applies to a single cavity (not recording a batch) when CAVITY_FDM_FUSED=1 or the
-// cavity's own choice (`want`, the autotuner's; -1 none) says so.  It is not the default: inside the step graph
-// it measured slower than six launches (C2 step 0.383 against 0.368 ms), the graph's programmatic launches
-// already hiding most of the gaps that the grid barriers replace.
-inline bool use_fused_pass(const FdmOperands& op, int want) {
-    (void)op;
-    if (g_launch_record || g_dgemm_tile == 64 || fused_pass_capacity() == 0) return false;
-    if (const char* e = std::getenv("CAVITY_FDM_FUSED")) return e[0] == '1';
-    return want == 1;
+// How a pass's six transforms are launched (CAVITY_FDM_FUSED, read when a solver or batch is created or a
+// standalone pass is called; else a cavity's autotuned choice; else -1: by size).
+//   kPassSix:        six launches of the tile GEMM;
+//   kPassOneLaunch:  one cooperative launch with grid barriers (single cavities only).  It is not a default: inside
+//                    the step graph it measured slower than six launches (C2 step 0.383 against 0.368 ms), the
+//                    graph's programmatic launches already hiding most of the gaps that the grid barriers replace;
+//   kPassPairs:      three launches of two chained transforms each, when no axis has more than 64 cells: the
+//                    default there.
+// A batch's launches follow the batch's choice (g_batch_pairs), the same for every member.
+enum PassForm : int { kPassSix = 0, kPassOneLaunch = 1, kPassPairs = 2 };
+inline int pass_form_from_env() {
+    const char* e = std::getenv("CAVITY_FDM_FUSED");
+    return e && *e ? std::atoi(e) : -1;
+}
+inline int pass_form(const FdmOperands& op, int want) {
+    const bool fits = pair_pass_fits(op.nx, op.ny, op.nz);
+    if (g_launch_record) return g_batch_pairs > 0 && fits ? kPassPairs : kPassSix;
+    const int f = want;
+    if (f == kPassOneLaunch) return g_dgemm_tile != 64 && fused_pass_capacity() > 0 ? kPassOneLaunch : kPassSix;
+    if (f == kPassSix) return kPassSix;
+    return fits ? kPassPairs : kPassSix;
 }
 
 inline void launch_fdm_pass(cudaStream_t st, const FdmOperands& op, const double* r, const double* r_alt, double* phi,
-                            double* t1, double* t2, Control* c, cudaGraphConditionalHandle h, bool clear, int fused = -1) {
-    if (use_fused_pass(op, fused)) {
+                            double* t1, double* t2, Control* c, cudaGraphConditionalHandle h, bool clear, int form = -1) {
+    const int f = pass_form(op, form);
+    if (f == kPassOneLaunch) {
         launch_fdm_pass_fused(st, op, r, r_alt, phi, t1, t2, c, h, clear);
+        return;
+    }
+    if (f == kPassPairs) {
+        launch_fdm_pass_pairs(st, op, r, r_alt, phi, t1, c, h, clear);
         return;
     }
     const int nx = op.nx, ny = op.ny, nz = op.nz, plane = nx * ny;

@@ -30,7 +30,8 @@ namespace cavity {
 // a batch of cavities collects every member's arguments for the same launch sequence this way and issues one
 // batched launch per entry.
 enum SweepKind : int { kSweepFace = 0, kSweepTile = 1, kSweepMarch = 2 };
-enum LaunchKind : int { kLkStepBegin = 0, kLkSweep, kLkStart, kLkResidual, kLkFinish, kLkDgemm64, kLkDgemm32, kLkTc };
+enum LaunchKind : int { kLkStepBegin = 0, kLkSweep, kLkStart, kLkResidual, kLkFinish, kLkDgemm64, kLkDgemm32, kLkTc,
+                        kLkPair };
 struct LaunchRecord {
     int kind, variant;
     dim3 grid;
@@ -42,6 +43,8 @@ inline thread_local std::vector<LaunchRecord>* g_launch_record = nullptr;
 inline thread_local int g_launch_batch = 1;
 // FP64 transform tile forced for every cavity of a batch whose cavities differ in size (0: chosen by size)
 inline thread_local int g_dgemm_tile = 0;
+// a batch's FP64 passes as three paired launches (1) or six (0); -1 outside a batch
+inline thread_local int g_batch_pairs = -1;
 // launch a step kernel with programmatic stream serialization (see pdl_wait); inside a stream capture this makes
 // the graph edge to the previous kernel a programmatic one
 template <class... KArgs, class... Args>

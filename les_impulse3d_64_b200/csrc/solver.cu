@@ -93,7 +93,7 @@ static long long estimate_bytes(const CavityConfig& c, int precision);
 struct Tuning {
     int chunks = 0;       // march sweep z-chunks (0: the device-filling rule)
     int dgemm = 0;        // FP64 transform tile, 32 or 64 (0: the size rule)
-    int fused = -1;       // FP64 pass as one cooperative launch: 1 yes, 0 no, -1 not chosen
+    int fused = -1;       // FP64 pass form (PassForm: 0 six launches, 1 one cooperative launch, 2 paired), -1 by size
     int sweep = -1;       // momentum sweep kernel (SweepKind; -1: not chosen)
     float ms = 0;         // measured step time of the choice
 };
@@ -645,7 +645,8 @@ public:
     // and keep the fastest (cached per grid size, stretching and precision; see Tuning).  Two rounds: first the
     // momentum sweep (the tile kernel, or the march with 1/2, 1, 2 and 4 times its device-filling z-chunk count;
     // only the chosen kernel when CAVITY_SWEEP names one), then, with the fastest sweep, the FP64 transforms where
-    // they run (64 x 64 tiles, 32 x 32 tiles, 32 x 32 tiles in one cooperative launch).
+    // they run (64 x 64 tiles, 32 x 32 tiles, 32 x 32 tiles in one cooperative launch, and three paired launches
+    // where no axis exceeds 64 cells).
     void autotune(int steps, int* chunks_out, int* dgemm_out, int* fused_out, float* ms_out) override {
         if (!pending_.empty()) fail("autotune: steps are queued; sync first");
         steps = std::max(steps, 2);
@@ -712,8 +713,9 @@ public:
         for (const Tuning& t : sweeps) consider(t);
         // round 2: the FP64 transforms, with that sweep
         if (!tc_fdm_ && best.ms > 0) {
-            std::vector<std::pair<int, int>> tiles = {{64, 0}, {32, 0}};
-            if (fused_pass_capacity() > 0) tiles.push_back({32, 1});
+            std::vector<std::pair<int, int>> tiles = {{64, kPassSix}, {32, kPassSix}};
+            if (fused_pass_capacity() > 0) tiles.push_back({32, kPassOneLaunch});
+            if (pair_pass_fits(nx_, ny_, nz_)) tiles.push_back({0, kPassPairs});
             const Tuning sw = best;
             for (const auto& t : tiles) {
                 Tuning cand = sw;
@@ -1050,7 +1052,8 @@ private:
         else {
             const int outer = g_dgemm_tile;              // a batch's choice wins over this cavity's own tuning
             if (!g_launch_record && tune_.dgemm) g_dgemm_tile = tune_.dgemm;
-            launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h != 0, tune_.fused);
+            launch_fdm_pass(st, fdm_, res_, rhs_, phi, t1_, t2_, ctrl_, h, use_h != 0,
+                            form_env_ >= 0 ? form_env_ : tune_.fused);
             g_dgemm_tile = outer;
         }
     }
@@ -1180,6 +1183,8 @@ private:
                 march_per_sm_ = std::max(1, march_per_sm_);
             }
             if (tc_fdm_) check(tc_transform_prepare());
+            check(pair_prepare());
+            form_env_ = pass_form_from_env();
         }
         for (cudaEvent_t& e : kev_) check(cudaEventCreate(&e));
         const char* env = std::getenv("CAVITY_GRAPHS");
@@ -1250,6 +1255,7 @@ private:
     bool sweep_forced_ = false;         // CAVITY_SWEEP named the kernel
     Tuning tune_;
     bool auto_tune_ = false;
+    int form_env_ = -1;                 // FP64 pass form named by CAVITY_FDM_FUSED at creation (-1: none)
     int march_per_sm_ = 1;
     // z-chunks of a march sweep launch: as many as fill the device's resident CTA slots once (all cavities of a
     // batch together) with at least four layers per chunk; CAVITY_MARCH_CHUNKS overrides
@@ -1349,6 +1355,14 @@ public:
         // cavities of different sizes share one FP64 transform tile: the large one when all of them together
         // have two 64 x 64 tiles per SM in the largest transform
         if (mixed_sizes_) dgemm_tile_ = tiles64 >= 2 * f.sms_ ? 64 : 32;
+        // FP64 passes as paired launches when every member's axes allow them (and CAVITY_FDM_FUSED names no
+        // other form)
+        {
+            bool fits = true;
+            for (const S_* s : m_) fits = fits && pair_pass_fits(s->nx_, s->ny_, s->nz_);
+            const int e = pass_form_from_env();
+            pairs_ = fits && (e < 0 || e == kPassPairs) ? 1 : 0;
+        }
         proto_ = m_[0];
         par_ = m_[0]->par_;
         nx_ = f.nx_;
@@ -1369,6 +1383,7 @@ public:
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)S_::MarchG::template smem_bytes<T>()));
         if (f.tc_fdm_) check(tc_transform_prepare_batched());
+        check(pair_prepare());
         for (int S = 0; S < 2; S++) build(S);
         proto_ = nullptr;        // members may leave and be destroyed from now on
     }
@@ -1444,7 +1459,7 @@ public:
             for (int S = 0; S < 2; S++) {
                 std::vector<LaunchRecord> rec;
                 {
-                    RecordGuard guard(&rec, (int)m_.size(), dgemm_tile_);
+                    RecordGuard guard(&rec, (int)m_.size(), dgemm_tile_, pairs_);
                     record_member(*s, S ^ d_[slot], S);
                 }
                 const Layout& L = layout_[S];
@@ -1469,15 +1484,17 @@ public:
 
 private:
     struct RecordGuard {
-        RecordGuard(std::vector<LaunchRecord>* r, int batch, int dgemm_tile) {
+        RecordGuard(std::vector<LaunchRecord>* r, int batch, int dgemm_tile, int pairs) {
             g_launch_record = r;
             g_launch_batch = batch;
             g_dgemm_tile = dgemm_tile;
+            g_batch_pairs = pairs;
         }
         ~RecordGuard() {
             g_launch_record = nullptr;
             g_launch_batch = 1;
             g_dgemm_tile = 0;
+            g_batch_pairs = -1;
         }
     };
     static size_t align256(size_t n) { return (n + 255) / 256 * 256; }
@@ -1530,7 +1547,7 @@ private:
         const size_t B = m_.size();
         std::vector<std::vector<LaunchRecord>> recs(B);
         for (size_t b = 0; b < B; b++) {
-            RecordGuard guard(&recs[b], (int)B, dgemm_tile_);
+            RecordGuard guard(&recs[b], (int)B, dgemm_tile_, pairs_);
             if (m_[b]) fn(*m_[b], (int)b);
             else fn(*proto_, 0);
         }
@@ -1610,6 +1627,7 @@ private:
                              live));
             break;
         case kLkTc: launch_tc_batched(r.variant, g, items, live, (const TcTransformArgs*)d, st); break;
+        case kLkPair: launch_pair_batched(r.variant, g, items, live, (const FdmPairArgs*)d, st); break;
         default: fail("batch: unknown launch");
         }
     }
@@ -1689,6 +1707,7 @@ private:
     std::vector<unsigned char> host_[2];      // host copies of the argument buffers
     Layout layout_[2];
     bool mixed_sizes_ = false;
+    int pairs_ = 0;             // FP64 passes as paired launches (every member's axes at most 64 cells)
     int dgemm_tile_ = 0;
     std::map<std::string, size_t> item_lists_;      // work lists already in the argument buffer, by content
 };
@@ -1787,7 +1806,8 @@ static void fdm_pass(int nx, int ny, int nz, const double* const s[3], const dou
     check(cudaMallocAsync((void**)&c, sizeof(Control), stream));
     const Control hc = standalone_fdm_control();
     check(cudaMemcpyAsync(c, &hc, sizeof hc, cudaMemcpyHostToDevice, stream));
-    launch_fdm_pass(stream, op, r, nullptr, phi, t1, t2, c, 0, false);
+    check(pair_prepare());
+    launch_fdm_pass(stream, op, r, nullptr, phi, t1, t2, c, 0, false, pass_form_from_env());
     const cudaError_t launched = cudaGetLastError();
     check(cudaFreeAsync(t1, stream));
     check(cudaFreeAsync(t2, stream));
@@ -1853,7 +1873,9 @@ static void fdm_pass_noalloc(int nx, int ny, int nz, const double* const s[3], c
     // the control block keeps the previous call's contents: reset its flags (error, reset) to zero
     const Control hc = standalone_fdm_control();
     check(cudaMemcpyAsync(scratch.control, &hc, sizeof hc, cudaMemcpyHostToDevice, stream));
-    launch_fdm_pass(stream, op, r, nullptr, phi, scratch.transforms, scratch.transforms + n, scratch.control, 0, false);
+    check(pair_prepare());
+    launch_fdm_pass(stream, op, r, nullptr, phi, scratch.transforms, scratch.transforms + n, scratch.control, 0, false,
+                    pass_form_from_env());
     check(cudaGetLastError());
     check(cudaStreamSynchronize(stream));
 }

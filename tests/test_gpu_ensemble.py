@@ -49,9 +49,8 @@ def test_many_mixed_cavities_set_up_and_converge():
 
 @pytest.mark.parametrize('group', ['precision', 'size'])
 def test_large_mixed_size_batch_matches_alone(group):
-    """48 cavities of three sizes in one batch: enough transform tiles that the batch runs the large FP64
-    transform tile, and few z-chunks per cavity in the column kernels, where a cavity alone fills the device with
-    its own.  Its reductions (norms, the mean of the potential) then add the same values in another grouping, so
+    """48 cavities of three sizes in one batch: few z-chunks per cavity in the column kernels, where a cavity alone
+    fills the device with its own.  Its reductions (norms, the mean of the potential) then add the same values in another grouping, so
     each cavity ends equal to itself alone to rounding: 1e-6 relative in the FP32 fields of the mixed form."""
     cases = workloads.ensemble_cases(count=48, seed=7, sizes=(16, 24, 32), re_range=(100.0, 2000.0))
     ens = Ensemble(cases, group=group)
@@ -71,3 +70,35 @@ def test_large_mixed_size_batch_matches_alone(group):
         for k in f:
             err = float(np.abs(f[k] - together[i][k]).max() / max(np.abs(f[k]).max(), 1e-30))
             assert err <= 1e-6, (i, k, err)
+
+
+@pytest.mark.parametrize('form', ['0', '2'])
+def test_batch_pass_forms_agree(form):
+    """A batch of cavities of three sizes with its FP64 passes as six launches (CAVITY_FDM_FUSED=0, the large and
+    the small transform tile) or as three paired launches (=2, the default when no axis exceeds 64 cells): the
+    same fields bit for bit as the default batch."""
+    import os
+    cases = workloads.ensemble_cases(count=12, seed=11, sizes=(16, 24, 40), re_range=(100.0, 2000.0))
+    for k, c in enumerate(cases):
+        c['precision'] = 'mixed' if k % 2 else 'fp64'
+
+    def run(env):
+        old = os.environ.pop('CAVITY_FDM_FUSED', None)
+        os.environ.update(env)
+        try:
+            ens = Ensemble(cases, group='precision')
+        finally:
+            os.environ.pop('CAVITY_FDM_FUSED', None)
+            if old is not None:
+                os.environ['CAVITY_FDM_FUSED'] = old
+        try:
+            ens.advance(3, chunk=3)
+            return [ens.fields(i) for i in range(len(cases))]
+        finally:
+            ens.close()
+
+    ref = run({})
+    got = run({'CAVITY_FDM_FUSED': form})
+    for i in range(len(cases)):
+        for k in ref[i]:
+            assert np.array_equal(ref[i][k], got[i][k]), (i, k)

@@ -51,11 +51,13 @@ def call_fdm(lib, name, S, inv_lambda, r, phi):
     return dphi.cpu().numpy()
 
 
-@pytest.mark.parametrize('fused', ['0', '1'])
-@pytest.mark.parametrize('dims', [(8, 8, 5), (24, 24, 16), (40, 40, 33), (64, 64, 64), (96, 80, 70)])
+@pytest.mark.parametrize('fused', ['0', '1', '2'])
+@pytest.mark.parametrize('dims', [(8, 8, 5), (7, 9, 11), (24, 24, 16), (40, 40, 33), (33, 64, 50), (64, 64, 64),
+                                  (96, 80, 70)])
 def test_fdm_pass_matches_numpy(dims, fused, monkeypatch):
-    """The FP64 pass as six launches (CAVITY_FDM_FUSED=0) and as one cooperative launch with grid barriers
-    between the transforms (=1), each against NumPy; and the two bit for bit against each other."""
+    """The FP64 pass as six launches (CAVITY_FDM_FUSED=0), as one cooperative launch with grid barriers between
+    the transforms (=1) and as three launches of two chained transforms each (=2, the default where no axis
+    exceeds 64 cells; six launches above), each against NumPy; and each bit for bit against the six launches."""
     monkeypatch.setenv('CAVITY_FDM_FUSED', fused)
     lib = load_library()
     lib.cavity_last_error.restype = ct.c_char_p
@@ -63,8 +65,66 @@ def test_fdm_pass_matches_numpy(dims, fused, monkeypatch):
     out = call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi)
     ref = fdm_reference(S, r, il, phi)
     assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
-    monkeypatch.setenv('CAVITY_FDM_FUSED', '1' if fused == '0' else '0')
+    monkeypatch.setenv('CAVITY_FDM_FUSED', '2' if fused == '0' else '0')
     assert np.array_equal(call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi), out)
+
+
+def test_fdm_pass_default_is_the_paired_pass(monkeypatch):
+    """Without CAVITY_FDM_FUSED a pass on axes of at most 64 cells is the paired one (bit for bit equal to it)."""
+    lib = load_library()
+    lib.cavity_last_error.restype = ct.c_char_p
+    S, il, r, phi = random_operands(48, 40, 36, seed=11)
+    monkeypatch.delenv('CAVITY_FDM_FUSED', raising=False)
+    out = call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi)
+    monkeypatch.setenv('CAVITY_FDM_FUSED', '2')
+    assert np.array_equal(call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi), out)
+
+
+FIELDS = ('u', 'v', 'w', 'mx', 'my', 'mz', 'phi')
+
+
+def solver_run(settings, precision, form, steps=3):
+    """`steps` steps of a random state, the solver created with CAVITY_FDM_FUSED=form (None: unset)."""
+    import os
+
+    from cases import random_state
+    from les_impulse3d_64_b200.api import Solver
+    old = os.environ.pop('CAVITY_FDM_FUSED', None)
+    if form is not None:
+        os.environ['CAVITY_FDM_FUSED'] = form
+    try:
+        sim = Solver(settings, precision=precision)
+    finally:
+        os.environ.pop('CAVITY_FDM_FUSED', None)
+        if old is not None:
+            os.environ['CAVITY_FDM_FUSED'] = old
+    try:
+        sim.initialize()
+        for name, a in random_state(sim.shapes, 9, True).items():
+            sim.set_field(name, a)
+        reps = [sim.step() for _ in range(steps)]
+        return reps, {k: sim.field64(k) for k in FIELDS}
+    finally:
+        sim.close()
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
+@pytest.mark.parametrize('grid', [dict(nx=16, ny=16, nz=8), dict(nx=22, ny=22, nz=9),
+                                  dict(nx=40, ny=40, nz=13, grid_stretch=1, grid_dx_wall=0.01),
+                                  dict(nx=64, ny=64, nz=64, grid_stretch=1, grid_dx_wall=0.0049)])
+def test_paired_pass_steps_equal_six_launch_steps(precision, grid):
+    """Whole steps (initial projection, refinement loops with their guess and pass decisions) with the paired
+    pass and with six launches per pass: the same reports and the same fields bit for bit."""
+    from cases import base_settings
+    s = base_settings(adaptive_dt=1, dt_max=0.01, nu=0.002, **grid)
+    rp, fp = solver_run(s, precision, '2')
+    rs, fs = solver_run(s, precision, '0')
+    rd, fd = solver_run(s, precision, None)
+    for a, b, c in zip(rp, rs, rd):
+        assert a == b == c
+    for k in FIELDS:
+        assert np.array_equal(fp[k], fs[k]), k
+        assert np.array_equal(fp[k], fd[k]), k
 
 
 @pytest.mark.parametrize('dims', [(8, 8, 5), (24, 24, 16), (40, 40, 33), (64, 64, 64), (128, 96, 130)])
