@@ -184,22 +184,26 @@ struct FdmPairArgs {
 
 __device__ __forceinline__ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-// dst[i * p + k] = src[i * ld + k] for i < rows, k < cols, and 0 elsewhere in the R x C extent (C even), as
-// cp.async copies of two doubles where alignment allows, else of one
+// dst[i * p + k] = src[i * ld + k] for i < rows, k < cols, and 0 elsewhere in the R x C extent (C even, at most
+// 2 LPR), as cp.async copies of two doubles where alignment allows, else of one.  LPR threads share a row, two
+// columns each, so the loop needs no index division.
+template <int LPR>
 __device__ __forceinline__ void pair_stage(double* dst, int p, const double* src, long long ld, int rows, int cols,
                                            int R, int C) {
-    const bool two = ld % 2 == 0 && ((unsigned long long)src & 15) == 0;
-    if (two) {
-        for (int e = threadIdx.x; e < R * C / 2; e += kPairThreads) {
-            const int i = e / (C / 2), k = 2 * (e % (C / 2));
-            const int n = i < rows ? min(2, max(0, cols - k)) : 0;
-            cp_async16z(&dst[i * p + k], n ? src + i * ld + k : src, 8 * n);
+    constexpr int RPS = kPairThreads / LPR;         // rows in flight per sweep of the block
+    const int k = 2 * (threadIdx.x % LPR);
+    if (k >= C) return;
+    const int n = min(2, max(0, cols - k));         // doubles of a row this thread copies (0: zero fill)
+    if (ld % 2 == 0 && ((unsigned long long)src & 15) == 0) {
+        for (int i = threadIdx.x / LPR; i < R; i += RPS) {
+            const int m = i < rows ? n : 0;
+            cp_async16z(&dst[i * p + k], m ? src + i * ld + k : src, 8 * m);
         }
     } else {
-        for (int e = threadIdx.x; e < R * C; e += kPairThreads) {
-            const int i = e / C, k = e % C;
-            const bool ok = i < rows && k < cols;
-            cp_async8(&dst[i * p + k], ok ? src + i * ld + k : src, ok ? 8 : 0);
+        for (int i = threadIdx.x / LPR; i < R; i += RPS) {
+            const bool ok = i < rows;
+            cp_async8(&dst[i * p + k], ok && n > 0 ? src + i * ld + k : src, ok && n > 0 ? 8 : 0);
+            cp_async8(&dst[i * p + k + 1], ok && n > 1 ? src + i * ld + k + 1 : src, ok && n > 1 ? 8 : 0);
         }
     }
 }
@@ -261,10 +265,10 @@ __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     const int nx = a.nx, ny = a.ny, z = blk.y, x0 = blk.x * W;
     const double* r = (a.r_alt && a.c->use_rhs ? a.r_alt : a.r) + (long long)z * nx * ny;
     const int my = round_up(ny, 8), kx = round_up(nx, 4), ky = round_up(ny, 4);
-    pair_stage(A1, kPairPitch, r, nx, ny, nx, my, round_up(kx, 2));
-    pair_stage(B1, PW, a.s[X] + x0, nx, nx, min(W, nx - x0), kx, W);
+    pair_stage<32>(A1, kPairPitch, r, nx, ny, nx, my, kx);
+    pair_stage<W / 2>(B1, PW, a.s[X] + x0, nx, nx, min(W, nx - x0), kx, W);
     cp_async_commit();
-    pair_stage(A2, kPairPitch, a.st[Y], ny, ny, ny, my, round_up(ky, 2));
+    pair_stage<32>(A2, kPairPitch, a.st[Y], ny, ny, ny, my, ky);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
@@ -307,10 +311,10 @@ __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     double* C1 = B1 + kPairMax * PW;
     const int nz = a.nz, plane = a.nx * a.ny, c0 = blk.x * W;
     const int mz = round_up(nz, 8), kz = round_up(nz, 4);
-    pair_stage(A1, kPairPitch, a.st[Z], nz, nz, nz, mz, round_up(kz, 2));
-    pair_stage(B1, PW, a.t + c0, plane, nz, min(W, plane - c0), kz, W);
+    pair_stage<32>(A1, kPairPitch, a.st[Z], nz, nz, nz, mz, kz);
+    pair_stage<W / 2>(B1, PW, a.t + c0, plane, nz, min(W, plane - c0), kz, W);
     cp_async_commit();
-    pair_stage(A2, kPairPitch, a.s[Z], nz, nz, nz, mz, round_up(kz, 2));
+    pair_stage<32>(A2, kPairPitch, a.s[Z], nz, nz, nz, mz, kz);
     cp_async_commit();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = warp * 8;
@@ -363,10 +367,10 @@ __device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     const int nx = a.nx, ny = a.ny, z = blk.y, y0 = blk.x * W;
     const int kx = round_up(nx, 4), ky = round_up(ny, 4), mx = round_up(nx, 8);
     const int cx = min(kPairMax, round_up(mx, 8 * FN));      // columns the active warps read: staged, zero past nx
-    pair_stage(A1, kPairPitch, a.s[Y] + (long long)y0 * ny, ny, min(W, ny - y0), ny, W, round_up(ky, 2));
-    pair_stage(B1, kPairPitch, a.t + (long long)z * nx * ny, nx, ny, nx, ky, cx);
+    pair_stage<32>(A1, kPairPitch, a.s[Y] + (long long)y0 * ny, ny, min(W, ny - y0), ny, W, ky);
+    pair_stage<32>(B1, kPairPitch, a.t + (long long)z * nx * ny, nx, ny, nx, ky, cx);
     cp_async_commit();
-    pair_stage(B2, kPairPitch, a.st[X], nx, nx, nx, kx, cx);
+    pair_stage<32>(B2, kPairPitch, a.st[X], nx, nx, nx, kx, cx);
     cp_async_commit();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = (warp / WN) * 8, n0 = (warp % WN) * FN * 8;    // the warp's 8 rows (y) x 8 FN columns (x)
@@ -410,20 +414,19 @@ template <int W> struct PairYxSmem {
     static constexpr size_t bytes = sizeof(double) * (2 * kPairMax * kPairPitch + 2 * W * kPairPitch);
 };
 
-constexpr int kPairW = 32;                   // columns (x, plane) or rows (y) of a paired-pass CTA
 enum PairPhase : int { kPairXy = 0, kPairZ = 1, kPairYx = 2 };
 
-__global__ void __launch_bounds__(kPairThreads, 2) pair_xy_kernel(FdmPairArgs a) {
-    pair_xy_body<kPairW>(a, real_blk(), first_block());
+template <int W> __global__ void __launch_bounds__(kPairThreads, 2) pair_xy_kernel(FdmPairArgs a) {
+    pair_xy_body<W>(a, real_blk(), first_block());
 }
-__global__ void __launch_bounds__(kPairThreads, 2) pair_z_kernel(FdmPairArgs a) {
-    pair_z_body<kPairW>(a, real_blk(), first_block());
+template <int W> __global__ void __launch_bounds__(kPairThreads, 2) pair_z_kernel(FdmPairArgs a) {
+    pair_z_body<W>(a, real_blk(), first_block());
 }
-__global__ void __launch_bounds__(kPairThreads, 2) pair_yx_kernel(FdmPairArgs a) {
-    pair_yx_body<kPairW>(a, real_blk(), first_block());
+template <int W> __global__ void __launch_bounds__(kPairThreads, 2) pair_yx_kernel(FdmPairArgs a) {
+    pair_yx_body<W>(a, real_blk(), first_block());
 }
 // a batch of cavities: grid x runs over the work list (BatchItem); the phase selects the body
-template <int PHASE>
+template <int PHASE, int W>
 __global__ void __launch_bounds__(kPairThreads, 2) pair_batched(const FdmPairArgs* args, const BatchItem* items,
                                                                const int* live) {
     __shared__ FdmPairArgs a;
@@ -434,43 +437,74 @@ __global__ void __launch_bounds__(kPairThreads, 2) pair_batched(const FdmPairArg
         return;
     }
     load_args(a, args + cav);
-    if (PHASE == kPairXy) pair_xy_body<kPairW>(a, k, first_block());
-    else if (PHASE == kPairZ) pair_z_body<kPairW>(a, k, first_block());
-    else pair_yx_body<kPairW>(a, k, first_block());
+    if (PHASE == kPairXy) pair_xy_body<W>(a, k, first_block());
+    else if (PHASE == kPairZ) pair_z_body<W>(a, k, first_block());
+    else pair_yx_body<W>(a, k, first_block());
 }
-inline size_t pair_smem_bytes(int phase) {
-    return phase == kPairYx ? PairYxSmem<kPairW>::bytes : PairSmem<kPairW>::bytes;
+inline size_t pair_smem_bytes(int phase, int w) {
+    if (w == 16) return phase == kPairYx ? PairYxSmem<16>::bytes : PairSmem<16>::bytes;
+    return phase == kPairYx ? PairYxSmem<32>::bytes : PairSmem<32>::bytes;
 }
-// grid of one phase for an nx x ny x nz cavity
-inline dim3 pair_grid(int phase, int nx, int ny, int nz) {
-    if (phase == kPairXy) return dim3((nx + kPairW - 1) / kPairW, nz);
-    if (phase == kPairZ) return dim3((nx * ny + kPairW - 1) / kPairW);
-    return dim3((ny + kPairW - 1) / kPairW, nz);
+// grid of one phase for an nx x ny x nz cavity with CTA width w
+inline dim3 pair_grid(int phase, int w, int nx, int ny, int nz) {
+    if (phase == kPairXy) return dim3((nx + w - 1) / w, nz);
+    if (phase == kPairZ) return dim3((nx * ny + w - 1) / w);
+    return dim3((ny + w - 1) / w, nz);
 }
 inline bool pair_pass_fits(int nx, int ny, int nz) {
     return nx <= kPairMax && ny <= kPairMax && nz <= kPairMax;
 }
+inline int current_sm_count() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return sms;
+}
+// CTA width: 32 columns (rows), or 16 when a single cavity's 32-wide grid leaves SMs without a CTA (more, smaller
+// CTAs: two per SM hide each other's latency).  A batch's launches all take 32.  CAVITY_PAIR_W=16 or 32 forces it.
+inline int pair_width(int nx, int nz) {
+    static const int forced = [] {
+        const char* e = std::getenv("CAVITY_PAIR_W");
+        return e ? std::atoi(e) : 0;
+    }();
+    static const int sms = current_sm_count();
+    if (forced == 16 || forced == 32) return forced;
+    if (g_launch_record) return 32;
+    const long long ctas = (long long)((nx + 31) / 32) * nz;
+    return ctas < sms ? 16 : 32;
+}
+template <int W> inline cudaError_t pair_prepare_w() {
+    cudaError_t r = cudaFuncSetAttribute(pair_xy_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pair_smem_bytes(kPairXy, W));
+    if (r == cudaSuccess)
+        r = cudaFuncSetAttribute(pair_z_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem_bytes(kPairZ, W));
+    if (r == cudaSuccess)
+        r = cudaFuncSetAttribute(pair_yx_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem_bytes(kPairYx, W));
+    if (r == cudaSuccess)
+        r = cudaFuncSetAttribute(pair_batched<kPairXy, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_smem_bytes(kPairXy, W));
+    if (r == cudaSuccess)
+        r = cudaFuncSetAttribute(pair_batched<kPairZ, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_smem_bytes(kPairZ, W));
+    if (r == cudaSuccess)
+        r = cudaFuncSetAttribute(pair_batched<kPairYx, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_smem_bytes(kPairYx, W));
+    return r;
+}
 // once per process, before any capture: the dynamic shared memory of the paired kernels
 inline cudaError_t pair_prepare() {
     static const cudaError_t e = [] {
-        cudaError_t r = cudaFuncSetAttribute(pair_xy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)pair_smem_bytes(kPairXy));
-        if (r == cudaSuccess)
-            r = cudaFuncSetAttribute(pair_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem_bytes(kPairZ));
-        if (r == cudaSuccess)
-            r = cudaFuncSetAttribute(pair_yx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem_bytes(kPairYx));
-        if (r == cudaSuccess)
-            r = cudaFuncSetAttribute(pair_batched<kPairXy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)pair_smem_bytes(kPairXy));
-        if (r == cudaSuccess)
-            r = cudaFuncSetAttribute(pair_batched<kPairZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)pair_smem_bytes(kPairZ));
-        if (r == cudaSuccess)
-            r = cudaFuncSetAttribute(pair_batched<kPairYx>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)pair_smem_bytes(kPairYx));
-        return r;
+        const cudaError_t r = pair_prepare_w<32>();
+        return r == cudaSuccess ? pair_prepare_w<16>() : r;
     }();
     return e;
+}
+template <int W>
+inline void launch_pair_w(int phase, dim3 grid, cudaStream_t st, const FdmPairArgs& a) {
+    const size_t smem = pair_smem_bytes(phase, W);
+    if (phase == kPairXy) launch_pdl(pair_xy_kernel<W>, grid, dim3(kPairThreads), smem, st, a);
+    else if (phase == kPairZ) launch_pdl(pair_z_kernel<W>, grid, dim3(kPairThreads), smem, st, a);
+    else launch_pdl(pair_yx_kernel<W>, grid, dim3(kPairThreads), smem, st, a);
 }
 inline void launch_fdm_pass_pairs(cudaStream_t st, const FdmOperands& op, const double* r, const double* r_alt,
                                   double* phi, double* t, const Control* c, cudaGraphConditionalHandle h, bool clear) {
@@ -480,20 +514,27 @@ inline void launch_fdm_pass_pairs(cudaStream_t st, const FdmOperands& op, const 
     for (int k = 0; k < 3; k++) { a.s[k] = op.s[k]; a.st[k] = op.st[k]; }
     a.inv_lambda = op.inv_lambda;
     a.r = r; a.r_alt = r_alt; a.t = t; a.phi = phi; a.c = c; a.handle = h;
-    void (*kernels[3])(FdmPairArgs) = {pair_xy_kernel, pair_z_kernel, pair_yx_kernel};
+    const int w = pair_width(op.nx, op.nz);
     for (int ph = 0; ph < 3; ph++) {
-        const dim3 grid = pair_grid(ph, op.nx, op.ny, op.nz);
-        if (!record_launch(kLkPair, ph, grid, pair_smem_bytes(ph), a))
-            launch_pdl(kernels[ph], grid, dim3(kPairThreads), pair_smem_bytes(ph), st, a);
+        const dim3 grid = pair_grid(ph, w, op.nx, op.ny, op.nz);
+        if (record_launch(kLkPair, ph | (w << 4), grid, pair_smem_bytes(ph, w), a)) continue;
+        if (w == 16) launch_pair_w<16>(ph, grid, st, a);
+        else launch_pair_w<32>(ph, grid, st, a);
     }
 }
-// a recorded paired launch (variant: the phase) over a batch of cavities
-inline void launch_pair_batched(int phase, dim3 grid, const BatchItem* items, const int* live, const FdmPairArgs* d,
+// a recorded paired launch (variant: phase | width << 4) over a batch of cavities
+template <int W>
+inline void launch_pair_batched_w(int phase, dim3 grid, const BatchItem* items, const int* live, const FdmPairArgs* d,
+                                  cudaStream_t st) {
+    const size_t smem = pair_smem_bytes(phase, W);
+    if (phase == kPairXy) launch_pdl(pair_batched<kPairXy, W>, grid, dim3(kPairThreads), smem, st, d, items, live);
+    else if (phase == kPairZ) launch_pdl(pair_batched<kPairZ, W>, grid, dim3(kPairThreads), smem, st, d, items, live);
+    else launch_pdl(pair_batched<kPairYx, W>, grid, dim3(kPairThreads), smem, st, d, items, live);
+}
+inline void launch_pair_batched(int variant, dim3 grid, const BatchItem* items, const int* live, const FdmPairArgs* d,
                                 cudaStream_t st) {
-    const size_t smem = pair_smem_bytes(phase);
-    if (phase == kPairXy) launch_pdl(pair_batched<kPairXy>, grid, dim3(kPairThreads), smem, st, d, items, live);
-    else if (phase == kPairZ) launch_pdl(pair_batched<kPairZ>, grid, dim3(kPairThreads), smem, st, d, items, live);
-    else launch_pdl(pair_batched<kPairYx>, grid, dim3(kPairThreads), smem, st, d, items, live);
+    if ((variant >> 4) == 16) launch_pair_batched_w<16>(variant & 15, grid, items, live, d, st);
+    else launch_pair_batched_w<32>(variant & 15, grid, items, live, d, st);
 }
 
 // ---------------------------------------------------------------------------------------------- one-launch pass

@@ -146,3 +146,38 @@ def test_fdm_pass_tf32_rejects_unaligned_rows():
     S, il, r, phi = random_operands(6, 6, 5, seed=3)
     with pytest.raises(RuntimeError, match='multiple of 4'):
         call_fdm(lib, 'cavity_fdm_pass_tf32', S, il, r, phi)
+
+
+WIDTH_CHECK = r'''
+import os, sys
+import numpy as np
+sys.path[:0] = [{tests!r}, {root!r}]
+import test_gpu_fdm as t
+from les_impulse3d_64_b200.api import load_library
+import ctypes as ct
+lib = load_library()
+lib.cavity_last_error.restype = ct.c_char_p
+for dims in ((8, 8, 5), (7, 9, 11), (40, 40, 33), (64, 64, 64)):
+    S, il, r, phi = t.random_operands(*dims, seed=sum(dims) + 5)
+    os.environ['CAVITY_FDM_FUSED'] = '2'
+    a = t.call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi)
+    os.environ['CAVITY_FDM_FUSED'] = '0'
+    b = t.call_fdm(lib, 'cavity_fdm_pass', S, il, r, phi)
+    assert np.array_equal(a, b), dims
+print('ok')
+'''
+
+
+@pytest.mark.parametrize('width', ['16', '32'])
+def test_paired_pass_widths(width):
+    """The paired pass with CTAs 16 or 32 columns wide (CAVITY_PAIR_W, read once per process: a child process
+    each) equals the six-launch pass bit for bit."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    tests = Path(__file__).resolve().parent
+    code = WIDTH_CHECK.format(tests=str(tests), root=str(tests.parent))
+    env = dict(os.environ, CAVITY_PAIR_W=width)
+    res = subprocess.run([sys.executable, '-c', code], env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0 and 'ok' in res.stdout, res.stdout + res.stderr
