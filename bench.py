@@ -224,18 +224,24 @@ def uses_tensor_cores(settings, precision):
     return precision == 'mixed' and settings['nx'] % 4 == 0 and (fdm == 'tc' or (fdm != 'dmma' and cells >= 1 << 21))
 
 
-def transforms_roofline(settings, ms_per_pass, tc, peak_gbs):
+def transforms_roofline(settings, ms_per_pass, tc, peak_gbs, launches=6):
     """The six transforms of a pressure pass: FLOP/s against the measured cuBLAS rate of their arithmetic (FP64
     DMMA against DGEMM; the mixed form's 3xTF32 tensor-core products, counted three times, against TF32 GEMM), and
-    bytes against HBM: 16 B per cell per transform (an 8-byte read and write; the first reads the FP64
-    residual, the last updates the FP64 potential) plus 8 B of 1/lambda."""
+    bytes against HBM.  Six launches move 16 B per cell per transform (an 8-byte read and write; the first reads
+    the FP64 residual, the last updates the FP64 potential) plus 8 B of 1/lambda; the three paired launches of
+    the FP64 pass (`launches` = 3) keep every second intermediate on chip: 8 B in and out each, 8 B of 1/lambda
+    and 8 B of the potential read."""
     nx, ny, nz = settings['nx'], settings['ny'], settings['nz']
     cells = nx * ny * nz
     flops = 4.0 * (nx + ny + nz) * cells * (3 if tc else 1)
-    nbytes = (6 * 16 + 8) * cells
+    paired = not tc and launches == 3
+    nbytes = (3 * 16 + 16 if paired else 6 * 16 + 8) * cells
     s = ms_per_pass / 1e3
     peak = gemm_peak_tflops('tf32' if tc else 'fp64')
-    return {'kernel': 'tc_transform_kernel (3xTF32)' if tc else 'dgemm_mma_kernel (FP64 DMMA)',
+    name = ('tc_transform_kernel (3xTF32)' if tc else
+            'pair_xy/pair_z/pair_yx_kernel (FP64 DMMA, two transforms per launch)' if paired else
+            'dgemm_mma_kernel (FP64 DMMA)')
+    return {'kernel': name, 'launches_per_pass': launches,
             'ms_per_pass': ms_per_pass, 'flops_per_pass': flops, 'achieved_tflops': flops / s / 1e12,
             'peak_tflops': peak, 'peak_kind': 'measured cuBLAS ' + ('TF32' if tc else 'DGEMM') + ' on this GPU',
             'tensor_frac': flops / s / 1e12 / peak, 'bytes_per_pass': nbytes, 'achieved_gbs': nbytes / s / 1e9,
@@ -358,7 +364,8 @@ def run_ours(args, ranks):
     ktimes = cav.kernel_times()
     passes = cav.pressure_passes() - passes0
     device_bytes = cav.device_bytes()
-    launches = args.steps * cav.kernels_per_step(0) + 7 * passes_in_timed(passes, args, cav)
+    per_pass = (cav.kernels_per_step(1) - cav.kernels_per_step(0)) // 3       # transforms + residual
+    launches = args.steps * cav.kernels_per_step(0) + per_pass * passes_in_timed(passes, args, cav)
     cav.close()
     total_ms = ranks.max(float(ms.sum()))
     value = replica_rate(ranks.world, cells, args.steps, total_ms)
@@ -424,7 +431,8 @@ def run_ours(args, ranks):
                      'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': profile_traffic(args.workload), 'ms_per_launch': kernel_s * 1e3},
         'stencil_kernels': cell_kernels,
-        'transforms': transforms_roofline(s, ranks.max(ktimes['transforms']) / 3, uses_tensor_cores(s, precision), peak),
+        'transforms': transforms_roofline(s, ranks.max(ktimes['transforms']) / 3, uses_tensor_cores(s, precision), peak,
+                                          per_pass - 1),
         'clocks': clocks.summary(),
     }
     if not args.no_batched and args.workload == 'c2_64cube_re1000':

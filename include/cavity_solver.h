@@ -103,14 +103,15 @@ int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, floa
 /* Autotuner (no counterpart in the reference): times `steps` whole steps from the current state under each
  * candidate, restoring the state after each, and keeps the fastest for this cavity, in two rounds: the momentum
  * sweep (the tile kernel, or the z-march with 1/2, 1, 2 or 4 times its device-filling z-chunk count; only the
- * kernel CAVITY_SWEEP names, when set), then the FP64 transforms (six launches of 64 x 64 or 32 x 32 tiles, or
- * one cooperative launch of 32 x 32 tiles).  The choice is cached per grid size, stretching and precision form
+ * kernel CAVITY_SWEEP names, when set), then the FP64 transforms (six launches of 64 x 64 or 32 x 32 tiles, one
+ * cooperative launch of 32 x 32 tiles, or, where no axis exceeds 64 cells, three launches of two chained
+ * transforms each).  The choice is cached per grid size, stretching and precision form
  * for the process, and in the file named by CAVITY_TUNE_FILE when that is set; cavities created later with the
  * same key start with it.  The transform choices and the chunk counts give bit-identical steps; the two sweep
  * kernels agree to rounding.  With CAVITY_AUTOTUNE=1 a cavity without a cached choice tunes itself (6 steps per
  * candidate) before its first step.  Outputs (each may be NULL): the chosen chunk count (0: the tile sweep),
- * tile (0: the size rule) and one-launch choice (1 yes, 0 no, -1 the size rule), and the step time in
- * milliseconds. */
+ * tile (0: the size rule) and pass form (0 six launches, 1 one cooperative launch, 2 three paired launches, -1
+ * the size rule), and the step time in milliseconds. */
 int cavity_autotune(CavitySolver* s, int steps, int* march_chunks, int* dgemm_tile, int* fused_pass, float* ms_per_step);
 /* After cavity_time_steps: ms[5] receives the mean device time per timed step (milliseconds, all three stages)
  * of the momentum sweeps, the projection starts, the residuals of their warm-start guesses, the finishes, and
@@ -125,7 +126,8 @@ int cavity_kernel_times(CavitySolver* s, double* ms);
 int cavity_eigenbasis(const CavityConfig* config, int axis, int on_gpu, double* lambda, double* S);
 /* The handle of the process-wide solver behind the solver_* functions (NULL if none). */
 CavitySolver* cavity_default(void);
-/* Number of kernels one step launches (fixed part plus per pressure pass) for the counts it reports. */
+/* Number of kernels one step launches (fixed part plus per pressure pass, for the cavity's transform launches) for
+ * the counts it reports. */
 int cavity_kernels_per_step(const CavitySolver* s, int phi_passes_per_stage);
 /* Queued steps with per-step outputs (no counterpart in the reference, whose run script makes a blocking
  * round trip per step for solver_probes and solver_add_statistics): queue `count` steps, each followed on the

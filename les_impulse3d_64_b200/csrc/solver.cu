@@ -595,7 +595,14 @@ public:
     long long device_bytes() const override { return arena_.bytes(); }
 
     // step begin; per stage the sweep, the projection start, the residual of its guess and the finish; 7 per pass
-    int kernels_per_step(int passes) const override { return 1 + 3 * 4 + 3 * passes * 7; }
+    // step begin, then per stage the sweep, the projection start, its guess's residual and the finish, and per pass
+    // the transforms' launches and the residual
+    int kernels_per_step(int passes) const override { return 1 + 3 * 4 + 3 * passes * (transform_launches() + 1); }
+    int transform_launches() const {
+        if (tc_fdm_) return 6;
+        const int f = pass_form(fdm_, form_env_ >= 0 ? form_env_ : tune_.fused);
+        return f == kPassPairs ? 3 : f == kPassOneLaunch ? 1 : 6;
+    }
     long long pressure_passes() const override { return hc_.pass_count; }
 
     // `steps` steps through the plain step graph, each timed by events around its launch; then, when `kms` is
