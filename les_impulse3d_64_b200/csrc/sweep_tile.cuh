@@ -4,9 +4,11 @@
 // input of the tile in shared memory first, all copies in flight at once (cp.async):
 //   - the velocity with the halos the 4th-order Lamb stencil reaches: 3 cells across a component's axis, 1-2
 //     along it;
-//   - the impulse with a 1-cell halo; stage 0 applies the gauge-reset blend m0 = r m + (1-r) u
-//     (backend.cu:880-881) while staging;
+//   - the impulse with a 1-cell halo; stage 0 then applies the gauge-reset blend m0 = r m + (1-r) u
+//     (backend.cu:880-881) in shared memory, its u values from the velocity boxes (which contain the impulse
+//     boxes' cells);
 //   - the slices of the per-axis coefficient tables the tile uses.
+// No thread waits on a global load while staging: every element is a cp.async, all in flight together.
 // Staged values outside the box are clamped copies; every stencil term that reaches them has weight zero.
 // K = u.m (backend.cu:218-222) is computed once per cell.  Each face then evaluates its eight edge terms
 // (vorticity times interpolated velocity: backend.cu:141-215) from shared memory and adds them in the
@@ -61,20 +63,23 @@ __device__ __forceinline__ int box_row_base(int row, int ys, int zs, int ex, int
 
 // Stage a W x H x D box of a face array whose x-extent is ex and corner x is xs, coordinates clamped into the
 // array, from the row offsets `rowbase` (box_row_base).  Each thread keeps one column (its x offset and clamp)
-// and steps through the rows NT / W at a time.  With `blend` the box receives r m + (1-r) u.
+// and steps through the rows NT / W at a time.
 template <class T, int W, int H, int D, int NT>
-__device__ __forceinline__ void stage_box(T* dst, const int* rowbase, const T* __restrict__ m, const T* __restrict__ u,
-                                          bool blend, T r, T omr, int xs, int ex) {
+__device__ __forceinline__ void stage_box(T* dst, const int* rowbase, const T* __restrict__ m, int xs, int ex) {
     constexpr int RPS = NT / W, ROWS = H * D;
     const int t = threadIdx.x;
     if (t >= RPS * W) return;
     const int ix = t % W;
     const int gx = clampi(xs + ix, 0, ex - 1);
-    for (int row = t / W; row < ROWS; row += RPS) {
-        const int gi = rowbase[row] + gx;
-        T* d = dst + row * W + ix;
-        if (blend) *d = r * m[gi] + omr * u[gi];
-        else cp_async_elem<sizeof(T)>(d, m + gi);
+    for (int row = t / W; row < ROWS; row += RPS) cp_async_elem<sizeof(T)>(dst + row * W + ix, m + rowbase[row] + gx);
+}
+// Stage 0's gauge-reset blend of a staged impulse box: m <- r m + (1-r) u, with u at the same face from the
+// velocity box (plane / row strides VP, VW; `uoff` its offset of the impulse box's corner)
+template <class T, int MW, int MH, int MD, int NT, int VW, int VP>
+__device__ __forceinline__ void blend_box(T* mb, const T* vb, int uoff, T r, T omr) {
+    for (int e = threadIdx.x; e < MW * MH * MD; e += NT) {
+        const int ix = e % MW, iy = (e / MW) % MH, iz = e / (MW * MH);
+        mb[e] = r * mb[e] + omr * vb[uoff + iz * VP + iy * VW + ix];
     }
 }
 
@@ -86,10 +91,11 @@ template <class T, int S> struct TabSlice {
 };
 
 // viscous flux-form Laplacian of the impulse at a face of component A from its staged box (strides 1, MW,
-// MW*MH), wall and lid fluxes, then the RK combination with the inviscid term L (backend.cu:289-329)
+// MW*MH), wall and lid fluxes, then the RK combination with the inviscid term L and the RK base value `base`
+// (stages 1, 2) (backend.cu:289-329)
 template <int A, class T, int MW, int MH, class TS0, class TS1, class TS2>
 __device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* mb, T wall, const StageConst& sc, T dt,
-                                             T lidv, int x, int y, int z, int i, T L, const TS0& ts0, const TS1& ts1,
+                                             T lidv, int x, int y, int z, T base, T L, const TS0& ts0, const TS1& ts1,
                                              const TS2& ts2) {
     const Params& p = a.p;
     const int q[3] = {x, y, z};
@@ -119,7 +125,7 @@ __device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* 
         lap = lap + (hi - lo) * tb(kInvW, q[t]);
     }
     T val = cc + dt * (a.nu * lap + L);
-    if (a.stage > 0) val = T(sc.a0) * a.m0[A][i] + T(sc.b) * val;
+    if (a.stage > 0) val = T(sc.a0) * base + T(sc.b) * val;
     return val;
 }
 
@@ -166,12 +172,12 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     }
     __syncthreads();
     const int* rbm = rowbase + RU + RV + RW;
-    stage_box<T, UW, UH, G::UD, NT>(SU, rowbase, a.u[X], nullptr, false, T(0), T(0), x0 - 1, nx + 1);
-    stage_box<T, VW, VH, G::VD, NT>(SV, rowbase + RU, a.u[Y], nullptr, false, T(0), T(0), x0 - 3, nx);
-    stage_box<T, WW, WH, G::WD, NT>(SW, rowbase + RU + RV, a.u[Z], nullptr, false, T(0), T(0), x0 - 3, nx);
-    stage_box<T, MW, MH, G::MD, NT>(MX, rbm, a.m[X], a.u[X], blend, a.r, a.one_minus_r, x0 - 1, nx + 1);
-    stage_box<T, MW, MH, G::MD, NT>(MY, rbm + RM, a.m[Y], a.u[Y], blend, a.r, a.one_minus_r, x0 - 1, nx);
-    stage_box<T, MW, MH, G::MD, NT>(MZ, rbm + 2 * RM, a.m[Z], a.u[Z], blend, a.r, a.one_minus_r, x0 - 1, nx);
+    stage_box<T, UW, UH, G::UD, NT>(SU, rowbase, a.u[X], x0 - 1, nx + 1);
+    stage_box<T, VW, VH, G::VD, NT>(SV, rowbase + RU, a.u[Y], x0 - 3, nx);
+    stage_box<T, WW, WH, G::WD, NT>(SW, rowbase + RU + RV, a.u[Z], x0 - 3, nx);
+    stage_box<T, MW, MH, G::MD, NT>(MX, rbm, a.m[X], x0 - 1, nx + 1);
+    stage_box<T, MW, MH, G::MD, NT>(MY, rbm + RM, a.m[Y], x0 - 1, nx);
+    stage_box<T, MW, MH, G::MD, NT>(MZ, rbm + 2 * RM, a.m[Z], x0 - 1, nx);
     for (int e = threadIdx.x; e < kNumTabs * (G::SX + G::SY + G::SZ); e += NT) {
         int k, i, axis, len, lo;
         if (e < kNumTabs * G::SX) { axis = X; k = e / G::SX; i = e % G::SX; len = G::SX; lo = x0; }
@@ -185,10 +191,16 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         const int n = axis == X ? nx : axis == Y ? ny : nz;
         const int idx = clampi(lo - 2 + i, -2, n + 2);
         T* dst = axis == X ? TXs : axis == Y ? TYs : TZs;
-        dst[k * len + i] = tab(g, axis, k, idx);
+        cp_async_elem<sizeof(T)>(dst + k * len + i, g.tab[axis] + k * g.stride[axis] + idx + kTabOffset);
     }
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
+    if (blend) {      // u of each impulse-box cell: the velocity box entry 2 cells further along its cross axes
+        blend_box<T, MW, MH, G::MD, NT, UW, UP>(MX, SU, (2 * UH + 2) * UW, a.r, a.one_minus_r);
+        blend_box<T, MW, MH, G::MD, NT, VW, VP>(MY, SV, 2 * VP + 2, a.r, a.one_minus_r);
+        blend_box<T, MW, MH, G::MD, NT, WW, WP>(MZ, SW, 2 * WW + 2, a.r, a.one_minus_r);
+        __syncthreads();
+    }
     const TabSlice<T, G::SX> tX{TXs, x0};
     const TabSlice<T, G::SY> tY{TYs, y0};
     const TabSlice<T, G::SZ> tZ{TZs, z0};
@@ -226,10 +238,15 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         const T* pw = SW + ((rz + 1) * WH + ry + 3) * WW + lane + 3;   // w at cells (x, y), z-face z
         const int mo = ((rz + 1) * MH + ry + 1) * MW + lane + 1;        // this cell's lower faces in the impulse boxes
         const T kc = Kc[kidx(lane + 1, ry + 1, rz + 1)];
+        // the RK base of the three faces (stages 1, 2), loaded here so that the faces' arithmetic hides the wait
+        const int iu = fidx<X>(p, x, y, z), iv = fidx<Y>(p, x, y, z), iw = fidx<Z>(p, x, y, z);
+        const bool rk = a.stage > 0;
+        const T bu = rk ? __ldg(a.m0[X] + iu) : T(0), bv = rk ? __ldg(a.m0[Y] + iv) : T(0),
+                bw = rk ? __ldg(a.m0[Z] + iw) : T(0);
 
         // ---------------- u-face x: z-edges (b = Y, omega_z) and y-edges (b = Z, omega_y)
         {
-            const int i = fidx<X>(p, x, y, z);
+            const int i = iu;
             if (blend) a.m0_out[X][i] = MX[mo];
             if (x == 0) a.out[X][i] = T(0);
             else {
@@ -268,7 +285,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                     L = L + c3 * (py3(2) + py3(-1));
                 }
                 L = L - (kc - Kc[kidx(lane, ry + 1, rz + 1)]) * tX(kInvSp, x);
-                a.out[X][i] = viscous_rk_tile<X, T, MW, MH>(a, MX + mo, pu[0], sc, dt, lidv, x, y, z, i, L, tX, tY, tZ);
+                a.out[X][i] = viscous_rk_tile<X, T, MW, MH>(a, MX + mo, pu[0], sc, dt, lidv, x, y, z, bu, L, tX, tY, tZ);
             }
             if (x == nx - 1) {
                 if (blend) a.m0_out[X][i + 1] = MX[mo + 1];
@@ -277,7 +294,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         }
         // ---------------- v-face y: z-edges (b = X, omega_z) and x-edges (b = Z, omega_x)
         {
-            const int i = fidx<Y>(p, x, y, z);
+            const int i = iv;
             if (blend) a.m0_out[Y][i] = MY[mo];
             if (y == 0) a.out[Y][i] = T(0);
             else {
@@ -316,7 +333,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                     L = L + c3 * (px3(2) + px3(-1));
                 }
                 L = L - (kc - Kc[kidx(lane + 1, ry, rz + 1)]) * tY(kInvSp, y);
-                a.out[Y][i] = viscous_rk_tile<Y, T, MW, MH>(a, MY + mo, pv[0], sc, dt, lidv, x, y, z, i, L, tX, tY, tZ);
+                a.out[Y][i] = viscous_rk_tile<Y, T, MW, MH>(a, MY + mo, pv[0], sc, dt, lidv, x, y, z, bv, L, tX, tY, tZ);
             }
             if (y == ny - 1) {
                 if (blend) a.m0_out[Y][i + nx] = MY[mo + MW];
@@ -325,7 +342,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         }
         // ---------------- w-face z: x-edges (b = Y, omega_x) and y-edges (b = X, omega_y)
         {
-            const int i = fidx<Z>(p, x, y, z);
+            const int i = iw;
             if (blend) a.m0_out[Z][i] = MZ[mo];
             if (z == 0) a.out[Z][i] = T(0);
             else {
@@ -364,7 +381,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                     L = L + c3 * (py3(2) + py3(-1));
                 }
                 L = L - (kc - Kc[kidx(lane + 1, ry + 1, rz)]) * tZ(kInvSp, z);
-                a.out[Z][i] = viscous_rk_tile<Z, T, MW, MH>(a, MZ + mo, pw[0], sc, dt, lidv, x, y, z, i, L, tX, tY, tZ);
+                a.out[Z][i] = viscous_rk_tile<Z, T, MW, MH>(a, MZ + mo, pw[0], sc, dt, lidv, x, y, z, bw, L, tX, tY, tZ);
             }
             if (z == nz - 1) {
                 if (blend) a.m0_out[Z][i + nx * ny] = MZ[mo + MW * MH];
