@@ -18,14 +18,17 @@
 // 4 consecutive k; cp.async copies of the basis image) while the tensor core works on panel p.  One
 // thread issues the tcgen05.mma.cta_group::1.kind::tf32 instructions (M = 128, N = BN, K = 8) and commits each
 // panel to that stage's mbarrier.  Every mbarrier wait is bounded: on time-out the kernel records
-// kDeviceWait in the control block, frees its TMEM and returns.  Only this kernel allocates TMEM, and the
-// shared memory of a CTA (>= 80 KB) keeps at most 2 CTAs of <= 64 columns on an SM, below its 512 columns.
+// kDeviceWait in the control block, frees its TMEM and returns.  Only this kernel and the staged one below
+// allocate TMEM, and their shared memory (>= 80 KB; 192 KB for the staged kernel's 128 columns) keeps at most two
+// CTAs of <= 64 columns, or one of 128, on an SM, below its 512 columns.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 #include "kernels.cuh"
 
@@ -451,6 +454,302 @@ __global__ void __launch_bounds__(kTcThreads) tc_transform_batched(const TcTrans
     tc_transform_body<BN, FA, F64>(g, k, first_block());
 }
 
+// ---------------------------------------------------------------- staged kernel
+// The same transform with the field brought in like the basis: every copy of a K panel (basis image and raw
+// field) is a cp.async issued NS - 1 panels ahead into a ring of NS shared-memory stages, and the field is split
+// into hi/lo in place once its panel has landed, so the K loop waits for no load.  256 threads share the copies
+// and the split; each thread's copy and split addresses are fixed for the whole K loop (only a panel offset
+// moves), so a panel costs a few instructions per element.  A CTA owns a 128 x BN tile.
+//  * field is A (x transforms): the raw fp32 values of 4 consecutive k of a row are one 16-byte copy into the
+//    hi image; the fp64 residual's (first transform) are two, into the hi and the lo image, scaled by 1/rms and
+//    rounded to float by the split;
+//  * field is B (y, z transforms: [k][n], n contiguous): one 4-byte copy per element into its K-major place, the
+//    lanes of a warp taking consecutive n of one k row.
+constexpr int kTc2Threads = 256;
+template <int BN, int NS> struct Tc2Smem {
+    static constexpr int kA = kTcRows * kTcKC * 4;      // bytes of one A panel part (hi or lo)
+    static constexpr int kB = BN * kTcKC * 4;
+    static constexpr int kStage = 2 * kA + 2 * kB;
+    static constexpr int kBytes = NS * kStage;
+};
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async16s(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ float4 ld_shared4(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ double2 ld_shared2d(uint32_t addr) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(addr));
+    return v;
+}
+// cp.async.wait_group with a run-time count of at most two groups still in flight
+__device__ __forceinline__ void cp_async_wait_le(int n) {
+    if (n <= 0) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    else if (n == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+}
+// byte offset of k within a 32-wide K panel's core-matrix rows (kmajor_off(r, k) - kmajor_off(r, 0))
+__host__ __device__ constexpr int kmajor_koff(int k) { return (k >> 2) * 128 + (k & 3) * 4; }
+
+template <int BN, int NS, int FA, int F64>
+__device__ void tc2_transform_body(const TcTransformArgs& g, const Blk& blk, bool first) {
+    static_assert(NS >= 2 && NS <= 3, "cp_async_wait_le covers at most two outstanding panels");
+    constexpr int NT = kTc2Threads;
+    static_assert(NT == 256 && (BN == 64 || BN == 128), "copy plans below assume 256 threads");
+    using L = Tc2Smem<BN, NS>;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[NS];
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+    const int b = blk.z;
+    const int m0 = blk.y * kTcRows, n0 = blk.x * BN;
+    const uint32_t sbase = smem_addr(smem);
+    pdl_launch_dependents();
+    if (warp == 0) tmem_alloc(&tmem_base, BN);
+    if (tid == 0) {
+        for (int s = 0; s < NS; s++) mbar_init(&mbar[s], 1);
+        failed = 0;
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    pdl_wait();
+    if (g.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(g.handle, 0u);
+    const Control* c = g.c;
+    const int err = c->error, use_rhs = c->use_rhs, reset = c->reset_phi, cond = c->cond;
+    const double rhs2 = c->rhs_norm2, res2 = c->res_norm2;
+    const double r2 = use_rhs ? rhs2 : res2;
+    if (err || !cond || !(r2 > 0)) {                       // no pass (backend.cu:803-804)
+        if (warp == 0) tmem_dealloc(tmem, BN);
+        return;
+    }
+    const double rms = sqrt(r2 / g.n_cell);
+    const double inv_rms = 1.0 / rms;
+    const float* F = F64 ? nullptr : g.field + b * g.field_bstride;
+    const double* Fd = F64 ? ((use_rhs && g.field64_alt) ? g.field64_alt : g.field64) + b * g.field_bstride : nullptr;
+    const int panels = (g.K + kTcKC - 1) / kTcKC;
+    const long long ld = g.field_ld;
+
+    // ---- copy plan, fixed over the K loop
+    // basis: rows [row0, row0 + BR) of a panel's images are BR * 128 contiguous bytes, 16 per copy
+    constexpr int BR = FA ? BN : kTcRows, BQ = BR * 8 / NT;
+    constexpr uint32_t kBasisDst = FA ? 2 * L::kA : 0, kBasisPart = FA ? L::kB : L::kA;
+    const long long bsrc0 = (long long)(FA ? n0 : m0) * kTcKC + tid * 4;       // floats, panel 0
+    const long long bstep = (long long)g.basis_rows * kTcKC;
+    // field as A: thread t copies rows r_t + 32 q (q < 4) at the 4 k of group k4_t (fa_item of t + 256 q)
+    const int fr_t = (tid & 7) + 8 * (warp >> 1), fk4_t = ((tid >> 3) & 3) + 4 * (warp & 1);
+    const uint32_t fa_off = kmajor_off(fr_t, 4 * fk4_t);
+    // field as B: thread t copies n = t % BN at k = h + S q (h = t / BN, S = 256 / BN)
+    constexpr int S = NT / BN, BQN = BN * kTcKC / NT;
+    const int bn_t = tid % BN, bh_t = tid / BN;
+    const uint32_t fb_off = 2 * L::kA + kmajor_off(bn_t, 0) + 4 * bh_t;
+    const bool fb_ok = n0 + bn_t < g.N;
+
+    auto issue = [&](int p, int s) {
+        const uint32_t st = sbase + s * L::kStage;
+        const int k0 = p * kTcKC;
+        const long long bsrc = bsrc0 + p * bstep;
+#pragma unroll
+        for (int q = 0; q < BQ; q++) {
+            cp_async16(st + kBasisDst + (tid + q * NT) * 16, g.basis_hi + bsrc + q * NT * 4);
+            cp_async16(st + kBasisDst + kBasisPart + (tid + q * NT) * 16, g.basis_lo + bsrc + q * NT * 4);
+        }
+        if (FA) {
+            const int k = k0 + 4 * fk4_t;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int gm = m0 + fr_t + 32 * q;
+                const bool ok = gm < g.M && k < g.K;
+                const uint32_t off = st + fa_off + q * 4096;
+                if (F64) {
+                    const double* src = Fd + gm * ld + k;
+                    cp_async16s(off, ok ? src : Fd, ok ? 16 : 0);
+                    cp_async16s(off + L::kA, ok ? src + 2 : Fd, ok ? 16 : 0);
+                } else {
+                    cp_async16s(off, ok ? F + gm * ld + k : F, ok ? 16 : 0);
+                }
+            }
+        } else {
+            const float* src = F + (long long)(k0 + bh_t) * ld + n0 + bn_t;
+#pragma unroll
+            for (int q = 0; q < BQN; q++) {
+                const bool ok = fb_ok && k0 + bh_t + S * q < g.K;
+                cp_async4(st + fb_off + kmajor_koff(S * q), ok ? src + S * q * ld : F, ok ? 4 : 0);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    // split the landed field of stage s in place: hi image <- TF32(x), lo image <- x - hi
+    auto split = [&](int s) {
+        const uint32_t st = sbase + s * L::kStage;
+        constexpr uint32_t part = FA ? L::kA : L::kB;
+#pragma unroll
+        for (int q = 0; q < (FA ? 4 : BN * 8 / NT); q++) {
+            const uint32_t off = FA ? st + fa_off + q * 4096
+                                    : st + 2 * L::kA + kmajor_off(bn_t, 0) + (bh_t + S * q) * 128;
+            float4 x;
+            if (F64) {
+                const double2 d01 = ld_shared2d(off), d23 = ld_shared2d(off + part);     // k, k+1 and k+2, k+3
+                x = make_float4((float)(d01.x * inv_rms), (float)(d01.y * inv_rms), (float)(d23.x * inv_rms),
+                                (float)(d23.y * inv_rms));
+            } else {
+                x = ld_shared4(off);
+            }
+            float h0, l0, h1, l1, h2, l2, h3, l3;
+            tf32_split(x.x, h0, l0);
+            tf32_split(x.y, h1, l1);
+            tf32_split(x.z, h2, l2);
+            tf32_split(x.w, h3, l3);
+            st_shared4(off, h0, h1, h2, h3);
+            st_shared4(off + part, l0, l1, l2, l3);
+        }
+    };
+
+    // the epilogue's other operand (phi or 1/lambda) comes into L2 while the panels are multiplied
+    {
+        const int row = m0 + (tid & 127), half = tid >> 7;
+        if (row < g.M && g.epilogue != kTcStore && !(g.epilogue == kTcAccumulate && reset)) {
+            const int c0 = n0 + half * (BN / 2);
+            const long long base = b * g.out_bstride + (long long)row * g.out_ld + c0;
+            const int cnt = min(BN / 2, g.N - c0);
+            const int esz = g.epilogue == kTcAccumulate ? 8 : 4;
+            const char* q = g.epilogue == kTcAccumulate ? (const char*)(g.phi + base) : (const char*)(g.inv_lambda + base);
+            for (int o = 0; o < cnt * esz; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + o));
+        }
+    }
+    const uint32_t idesc = umma_idesc_tf32(kTcRows, BN, 0, 0);
+    int issued = 0;
+    for (; issued < panels && issued < NS; issued++) issue(issued, issued);
+    for (int p = 0; p < panels; p++) {
+        const int s = p % NS;
+        cp_async_wait_le(issued - p - 1);                  // this thread's copies of panel p have landed
+        __syncthreads();                                    // ... and every thread's
+        split(s);
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t st = sbase + s * L::kStage;
+            const uint32_t a_hi = st, a_lo = st + L::kA, b_hi = st + 2 * L::kA, b_lo = b_hi + L::kB;
+#pragma unroll
+            for (int ks = 0; ks < kTcKC / 8; ks++) {
+                const uint64_t ah = umma_desc(a_hi + ks * 256, kKmajorLBO, kKmajorSBO);
+                const uint64_t al = umma_desc(a_lo + ks * 256, kKmajorLBO, kKmajorSBO);
+                const uint64_t bh = umma_desc(b_hi + ks * 256, kKmajorLBO, kKmajorSBO);
+                const uint64_t bl = umma_desc(b_lo + ks * 256, kKmajorLBO, kKmajorSBO);
+                umma_tf32(tmem, al, bh, idesc, (p > 0 || ks > 0) ? 1u : 0u);
+                umma_tf32(tmem, ah, bl, idesc, 1u);
+                umma_tf32(tmem, ah, bh, idesc, 1u);
+            }
+            umma_commit(&mbar[s]);
+        }
+        // the stage of panel p - 1 is free once its MMAs are done: it takes the next panel
+        if (p >= 1 && issued < panels) {
+            const int q = p - 1;
+            if (!mbar_wait_bounded(&mbar[q % NS], (q / NS) & 1)) failed = 1;
+            __syncthreads();
+            if (failed) break;
+            issue(issued, issued % NS);
+            issued++;
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (!failed && !mbar_wait_bounded(&mbar[(panels - 1) % NS], ((panels - 1) / NS) & 1)) failed = 1;
+    tc_fence_after();
+    __syncthreads();
+    if (failed) {
+        if (tid == 0) atomicExch(g.error, (int)kDeviceWait);
+        tc_fence_before();
+        __syncthreads();
+        if (warp == 0) tmem_dealloc(tmem, BN);
+        return;
+    }
+    // epilogue through shared memory: warp w moves TMEM lanes 32 (w % 4) .. + 31, columns of half w / 4, into a
+    // row-major tile (pitch BN + 4 floats); then every warp writes 16 whole rows back, row-contiguous
+    constexpr int kPitch = BN + 4;
+    static_assert(kTcRows * kPitch * 4 <= L::kBytes, "epilogue tile exceeds the stages");
+    float* tile = reinterpret_cast<float*>(smem);
+    {
+        const int lb = warp & 3, half = warp >> 2;
+#pragma unroll 1
+        for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(lb * 32) << 16) + c0, v);
+            float* dst = tile + (lb * 32 + lane) * kPitch + c0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                *reinterpret_cast<float4*>(dst + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        }
+    }
+    __syncthreads();
+    constexpr int kLanesPerRow = BN / 4, kRowsPerStep = 32 / kLanesPerRow;
+    const int lr = lane / kLanesPerRow, lc = (lane % kLanesPerRow) * 4;
+    const int gcol = n0 + lc;
+#pragma unroll 2
+    for (int r0 = 0; r0 < kTcRows / 8; r0 += kRowsPerStep) {
+        const int rl = warp * (kTcRows / 8) + r0 + lr, grow = m0 + rl;
+        if (grow >= g.M || gcol >= g.N) continue;          // N is a multiple of 4: a float4 is all in or out
+        float4 x = *reinterpret_cast<const float4*>(tile + rl * kPitch + lc);
+        const long long idx = b * g.out_bstride + (long long)grow * g.out_ld + gcol;
+        if (g.epilogue == kTcAccumulate) {
+            double2 p0 = make_double2(0.0, 0.0), p1 = make_double2(0.0, 0.0);
+            if (!reset) {
+                p0 = *reinterpret_cast<const double2*>(g.phi + idx);
+                p1 = *reinterpret_cast<const double2*>(g.phi + idx + 2);
+            }
+            p0.x += (double)x.x * rms; p0.y += (double)x.y * rms;
+            p1.x += (double)x.z * rms; p1.y += (double)x.w * rms;
+            *reinterpret_cast<double2*>(g.phi + idx) = p0;
+            *reinterpret_cast<double2*>(g.phi + idx + 2) = p1;
+        } else {
+            if (g.epilogue == kTcScaleInvLambda) {
+                const float4 il = *reinterpret_cast<const float4*>(g.inv_lambda + idx);
+                x.x *= il.x; x.y *= il.y; x.z *= il.z; x.w *= il.w;
+            }
+            *reinterpret_cast<float4*>(g.out + idx) = x;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, BN);
+}
+
+// tile width and ring depth of the staged kernel (compile-time; -DCAVITY_TC2_BN / -DCAVITY_TC2_NS override)
+#ifndef CAVITY_TC2_BN
+#define CAVITY_TC2_BN 128
+#endif
+#ifndef CAVITY_TC2_NS
+#define CAVITY_TC2_NS 3
+#endif
+constexpr int kTc2BN = CAVITY_TC2_BN, kTc2NS = CAVITY_TC2_NS;
+constexpr int kTcStagedVariant = 1 << 10;      // flag of a recorded launch of the staged kernel
+template <int FA, int F64>
+__global__ void __launch_bounds__(kTc2Threads) tc2_transform_kernel(TcTransformArgs g) {
+    tc2_transform_body<kTc2BN, kTc2NS, FA, F64>(g, real_blk(), first_block());
+}
+template <int FA, int F64>
+__global__ void __launch_bounds__(kTc2Threads) tc2_transform_batched(const TcTransformArgs* args, const BatchItem* items,
+                                                                     const int* live) {
+    __shared__ TcTransformArgs g;
+    int cav;
+    const Blk k = item_blk(items, live, cav);
+    if (cav < 0) {
+        dead_slot_clear(args, items);
+        return;
+    }
+    load_args(g, args + cav);
+    tc2_transform_body<kTc2BN, kTc2NS, FA, F64>(g, k, first_block());
+}
+
 // ---------------------------------------------------------------- host side
 // tile width: 64 columns when that still gives one CTA per SM, else 32.  (128-column tiles would need 128 KB of
 // shared memory, one CTA per SM, and each CTA's K loop is latency-bound: two CTAs per SM of 64 columns are faster.)
@@ -481,9 +780,20 @@ template <int BN> inline cudaError_t tc_prepare_batched_bn() {
                                  TcSmem<BN>::kBytes);
     return e;
 }
+inline cudaError_t tc2_prepare() {
+    constexpr int bytes = Tc2Smem<kTc2BN, kTc2NS>::kBytes;
+    cudaError_t e = cudaFuncSetAttribute(tc2_transform_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tc2_transform_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tc2_transform_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tc2_transform_batched<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tc2_transform_batched<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(tc2_transform_batched<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
 inline cudaError_t tc_transform_prepare_batched() {
     cudaError_t e = tc_prepare_batched_bn<64>();
     if (e == cudaSuccess) e = tc_prepare_batched_bn<32>();
+    if (e == cudaSuccess) e = tc2_prepare();
     return e;
 }
 template <int BN>
@@ -498,12 +808,21 @@ inline void launch_tc_batched_bn(int fa, int f64, dim3 grid, const BatchItem* it
 inline void launch_tc_batched(int variant, dim3 grid, const BatchItem* items, const int* live, const TcTransformArgs* d,
                               cudaStream_t st) {
     const int bn = variant & 0xff, fa = (variant >> 8) & 1, f64 = (variant >> 9) & 1;
+    if (variant & kTcStagedVariant) {
+        constexpr int bytes = Tc2Smem<kTc2BN, kTc2NS>::kBytes;
+        const dim3 block(kTc2Threads);
+        if (fa && f64) launch_pdl(tc2_transform_batched<1, 1>, grid, block, bytes, st, d, items, live);
+        else if (fa) launch_pdl(tc2_transform_batched<1, 0>, grid, block, bytes, st, d, items, live);
+        else launch_pdl(tc2_transform_batched<0, 0>, grid, block, bytes, st, d, items, live);
+        return;
+    }
     if (bn == 64) launch_tc_batched_bn<64>(fa, f64, grid, items, live, d, st);
     else launch_tc_batched_bn<32>(fa, f64, grid, items, live, d, st);
 }
 inline cudaError_t tc_transform_prepare() {
     cudaError_t e = tc_prepare_bn<64>();
     if (e == cudaSuccess) e = tc_prepare_bn<32>();
+    if (e == cudaSuccess) e = tc2_prepare();
     return e;
 }
 template <int BN> inline void launch_tc_bn(cudaStream_t st, const TcTransformArgs& g, dim3 grid) {
@@ -514,7 +833,32 @@ template <int BN> inline void launch_tc_bn(cudaStream_t st, const TcTransformArg
 }
 // variant code of a recorded launch: tile width, field-is-A, fp64 field
 inline int tc_variant(int bn, const TcTransformArgs& g) { return bn | (g.field_is_a ? 1 << 8 : 0) | (g.field64 ? 1 << 9 : 0); }
+// The staged kernel (tc2_transform_body) for a single cavity's launch whose 128 x 128 tiles fit on the SMs at
+// once (one CTA per SM): there its deeper prefetch shortens the one CTA chain the launch lasts (C3 pass 84 against
+// 88 us).  With more tiles than SMs, and in batches, the register-pipelined kernel, whose two CTAs per SM overlap
+// each other's latencies (C6 pass 860 against 872 us).  CAVITY_TC_KERNEL=staged or =panel forces either.
+inline bool tc_use_staged(const TcTransformArgs& g, int batch, int sms) {
+    static const int forced = [] {
+        const char* e = std::getenv("CAVITY_TC_KERNEL");
+        if (!e) return -1;
+        return std::string(e) == "staged" ? 1 : std::string(e) == "panel" ? 0 : -1;
+    }();
+    if (forced >= 0) return forced == 1;
+    if (g_launch_record) return false;
+    const long long tiles = (long long)((g.N + kTc2BN - 1) / kTc2BN) * ((g.M + kTcRows - 1) / kTcRows) * batch;
+    return tiles <= sms;
+}
 inline void launch_tc_transform(cudaStream_t st, const TcTransformArgs& g, int batch, int sms) {
+    if (tc_use_staged(g, batch, sms)) {
+        const dim3 grid((g.N + kTc2BN - 1) / kTc2BN, (g.M + kTcRows - 1) / kTcRows, batch);
+        constexpr int bytes = Tc2Smem<kTc2BN, kTc2NS>::kBytes;
+        if (record_launch(kLkTc, tc_variant(kTc2BN, g) | kTcStagedVariant, grid, (size_t)bytes, g)) return;
+        const dim3 block(kTc2Threads);
+        if (g.field_is_a && g.field64) launch_pdl(tc2_transform_kernel<1, 1>, grid, block, bytes, st, g);
+        else if (g.field_is_a) launch_pdl(tc2_transform_kernel<1, 0>, grid, block, bytes, st, g);
+        else launch_pdl(tc2_transform_kernel<0, 0>, grid, block, bytes, st, g);
+        return;
+    }
     const int bn = tc_pick_bn(g.M, g.N, batch * g_launch_batch, sms);
     const dim3 grid((g.N + bn - 1) / bn, (g.M + kTcRows - 1) / kTcRows, batch);
     if (record_launch(kLkTc, tc_variant(bn, g), grid, (size_t)(bn == 64 ? TcSmem<64>::kBytes : TcSmem<32>::kBytes), g))

@@ -181,3 +181,41 @@ def test_paired_pass_widths(width):
     env = dict(os.environ, CAVITY_PAIR_W=width)
     res = subprocess.run([sys.executable, '-c', code], env=env, capture_output=True, text=True, timeout=300)
     assert res.returncode == 0 and 'ok' in res.stdout, res.stdout + res.stderr
+
+
+TC_KERNEL_RUN = r'''
+import sys
+import numpy as np
+sys.path[:0] = [{tests!r}, {root!r}]
+import test_gpu_fdm as t
+from les_impulse3d_64_b200.api import load_library
+import ctypes as ct
+lib = load_library()
+lib.cavity_last_error.restype = ct.c_char_p
+out = {{}}
+for dims in ((8, 8, 5), (24, 24, 16), (40, 40, 33), (128, 96, 130), (132, 20, 36)):
+    S, il, r, phi = t.random_operands(*dims, seed=sum(dims) + 7)
+    out['x'.join(map(str, dims))] = t.call_fdm(lib, 'cavity_fdm_pass_tf32', S, il, r, phi)
+np.savez({path!r}, **out)
+'''
+
+
+def test_tc_kernels_agree(tmp_path):
+    """The two tensor-core transform kernels, the register-pipelined one and the staged one (CAVITY_TC_KERNEL
+    selects, read once per process: a child process each), give the same pass bit for bit: the same split
+    operands and the same MMA sequence for every output element, whatever the tile width."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    tests = Path(__file__).resolve().parent
+    res = {}
+    for kind in ('staged', 'panel'):
+        path = str(tmp_path / f'{kind}.npz')
+        code = TC_KERNEL_RUN.format(tests=str(tests), root=str(tests.parent), path=path)
+        env = dict(os.environ, CAVITY_TC_KERNEL=kind)
+        r = subprocess.run([sys.executable, '-c', code], env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        res[kind] = dict(np.load(path))
+    for k in res['panel']:
+        assert np.array_equal(res['staged'][k], res['panel'][k]), k
