@@ -236,10 +236,14 @@ __device__ __forceinline__ void pair_warp_mma(double (&acc)[FM][FN][2], const do
 
 // The pass's entry checks (as dgemm_mma_body's): programmatic launch, the loop guard, error and residual.
 // False when the block has nothing to do.
-__device__ __forceinline__ bool pair_enter(const FdmPairArgs& a, bool first, bool clear) {
+// Each kernel issues the copies that do not depend on the control block before reading it, so that their
+// latencies overlap; a block with nothing to do waits for its copies to land before it exits.
+__device__ __forceinline__ void pair_begin(const FdmPairArgs& a, bool first, bool clear) {
     pdl_launch_dependents();
     pdl_wait();
     if (clear && a.clear_condition && threadIdx.x == 0 && first) cudaGraphSetConditional(a.handle, 0u);
+}
+__device__ __forceinline__ bool pair_live(const FdmPairArgs& a) {
     const Control* c = a.c;
     if (c->error || !c->cond) return false;
     const double r2 = c->use_rhs ? c->rhs_norm2 : c->res_norm2;
@@ -255,7 +259,7 @@ template <int W> struct PairSmem {
 // t[z] = ST_y (r[z] S_x) on columns [x0, x0 + W) of plane z: transforms 1 and 2 of the pass
 template <int W>
 __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
-    if (!pair_enter(a, first, true)) return;
+    pair_begin(a, first, true);
     constexpr int PW = PairSmem<W>::kPanel, FN = W / 8;
     extern __shared__ __align__(16) double pair_smem[];
     double* A1 = pair_smem;                         // r[z]: ny x nx
@@ -263,14 +267,18 @@ __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     double* B1 = A2 + kPairMax * kPairPitch;        // S_x[:, x0 .. x0 + W)
     double* C1 = B1 + kPairMax * PW;                // r[z] S_x on those columns
     const int nx = a.nx, ny = a.ny, z = blk.y, x0 = blk.x * W;
-    const double* r = (a.r_alt && a.c->use_rhs ? a.r_alt : a.r) + (long long)z * nx * ny;
     const int my = round_up(ny, 8), kx = round_up(nx, 4), ky = round_up(ny, 4);
-    pair_stage<32>(A1, kPairPitch, r, nx, ny, nx, my, kx);
     pair_stage<W / 2>(B1, PW, a.s[X] + x0, nx, nx, min(W, nx - x0), kx, W);
-    cp_async_commit();
     pair_stage<32>(A2, kPairPitch, a.st[Y], ny, ny, ny, my, ky);
     cp_async_commit();
-    cp_async_wait<1>();
+    if (!pair_live(a)) {
+        cp_async_wait<0>();
+        return;
+    }
+    const double* r = (a.r_alt && a.c->use_rhs ? a.r_alt : a.r) + (long long)z * nx * ny;
+    pair_stage<32>(A1, kPairPitch, r, nx, ny, nx, my, kx);
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = warp * 8;                        // the warp's 8 rows (y) x W columns
@@ -283,7 +291,6 @@ __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
             C1[(m0 + fr) * PW + j * 8 + 2 * fc + 1] = acc[0][j][1];
         }
     }
-    cp_async_wait<0>();
     __syncthreads();
     if (m0 >= my) return;
     pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, ky, m0, 0);
@@ -302,7 +309,7 @@ __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
 // t[:, c] = S_z (inv_lambda .* (ST_z t[:, c])) on plane columns c in [c0, c0 + W), in place: transforms 3 and 4
 template <int W>
 __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
-    if (!pair_enter(a, first, false)) return;
+    pair_begin(a, first, false);
     constexpr int PW = PairSmem<W>::kPanel, FN = W / 8;
     extern __shared__ __align__(16) double pair_smem[];
     double* A1 = pair_smem;                         // ST_z
@@ -316,6 +323,10 @@ __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     cp_async_commit();
     pair_stage<32>(A2, kPairPitch, a.s[Z], nz, nz, nz, mz, kz);
     cp_async_commit();
+    if (!pair_live(a)) {
+        cp_async_wait<0>();
+        return;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = warp * 8;
     double acc[1][FN][2], il[FN][2];
@@ -357,7 +368,7 @@ __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
 // phi[z] += (S_y t[z]) ST_x on rows [y0, y0 + W) of plane z: transforms 5 and 6
 template <int W>
 __device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
-    if (!pair_enter(a, first, false)) return;
+    pair_begin(a, first, false);
     constexpr int WN = 8 / (W / 8), FN = kPairMax / 8 / WN;   // warps along x, fragments per warp along x
     extern __shared__ __align__(16) double pair_smem[];
     double* B1 = pair_smem;                         // t[z]: ny x nx
@@ -372,6 +383,10 @@ __device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     cp_async_commit();
     pair_stage<32>(B2, kPairPitch, a.st[X], nx, nx, nx, kx, cx);
     cp_async_commit();
+    if (!pair_live(a)) {
+        cp_async_wait<0>();
+        return;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = (warp / WN) * 8, n0 = (warp % WN) * FN * 8;    // the warp's 8 rows (y) x 8 FN columns (x)
     const bool active = n0 < mx;

@@ -137,7 +137,6 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
     constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
     constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;      // plane strides of the velocity boxes
-    if (a.c->error) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* SU = reinterpret_cast<T*>(smem_raw);
     T* SV = SU + G::NU;
@@ -193,8 +192,14 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         T* dst = axis == X ? TXs : axis == Y ? TYs : TZs;
         cp_async_elem<sizeof(T)>(dst + k * len + i, g.tab[axis] + k * g.stride[axis] + idx + kTabOffset);
     }
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // the control block's values, read while the copies are in flight
+    const int failed = a.c->error;
+    const StageConst sc = stage_const(a.stage, a.c);
+    const T dt = (T)a.c->dt;
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
+    if (failed) return;
     if (blend) {      // u of each impulse-box cell: the velocity box entry 2 cells further along its cross axes
         blend_box<T, MW, MH, G::MD, NT, UW, UP>(MX, SU, (2 * UH + 2) * UW, a.r, a.one_minus_r);
         blend_box<T, MW, MH, G::MD, NT, VW, VP>(MY, SV, 2 * VP + 2, a.r, a.one_minus_r);
@@ -218,8 +223,6 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     }
     __syncthreads();
 
-    const StageConst sc = stage_const(a.stage, a.c);
-    const T dt = (T)a.c->dt;
     const T lidv = (T)lid_speed(p, sc.tau);
     const T half = T(0.5), eighth = T(0.125);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
