@@ -129,30 +129,40 @@ __device__ __forceinline__ T viscous_rk_tile(const MomentumArgs<T>& a, const T* 
     return val;
 }
 
+// The shared-memory arrays of a tile (in this order from the start of dynamic shared memory)
+template <class T> struct TileArrays {
+    T *SU, *SV, *SW, *MX, *MY, *MZ, *Kc, *TXs, *TYs, *TZs;
+};
+template <class T, class G> __device__ __forceinline__ TileArrays<T> tile_arrays(unsigned char* base) {
+    TileArrays<T> t;
+    t.SU = reinterpret_cast<T*>(base);
+    t.SV = t.SU + G::NU;
+    t.SW = t.SV + G::NV;
+    t.MX = t.SW + G::NW;
+    t.MY = t.MX + G::NM;
+    t.MZ = t.MY + G::NM;
+    t.Kc = t.MZ + G::NM;
+    t.TXs = t.Kc + G::NK;
+    t.TYs = t.TXs + kNumTabs * G::SX;
+    t.TZs = t.TYs + kNumTabs * G::SY;
+    return t;
+}
+
+// Everything a tile's faces need before their arithmetic: the staged boxes and table slices, stage 0's blend, K
+// per cell, and the stage constants.  False (in every thread) when the step has failed.
 template <class T, int TY, int TZ, int NT>
-__device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
+__device__ bool tile_prologue(const MomentumArgs<T>& a, const Blk& blk, const TileArrays<T>& t, StageConst& sc, T& dt) {
     using G = TileGeom<TY, TZ, NT>;
     pdl_launch_dependents();
     pdl_wait();
-    constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
+    constexpr int TX = G::TX;
     constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
     constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;      // plane strides of the velocity boxes
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* SU = reinterpret_cast<T*>(smem_raw);
-    T* SV = SU + G::NU;
-    T* SW = SV + G::NV;
-    T* MX = SW + G::NW;
-    T* MY = MX + G::NM;
-    T* MZ = MY + G::NM;
-    T* Kc = MZ + G::NM;
-    T* TXs = Kc + G::NK;
-    T* TYs = TXs + kNumTabs * G::SX;
-    T* TZs = TYs + kNumTabs * G::SY;
+    T *SU = t.SU, *SV = t.SV, *SW = t.SW, *MX = t.MX, *MY = t.MY, *MZ = t.MZ, *Kc = t.Kc;
     const Params& p = a.p;
     const Geo<T>& g = a.g;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int x0 = blk.x * TX, y0 = blk.y * TY, z0 = blk.z * TZ;
-    const int o4 = p.o4;
     const bool blend = a.stage == 0;
 
     // ---- stage: row offsets of the six boxes first (one pass), then every box
@@ -189,26 +199,23 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         }
         const int n = axis == X ? nx : axis == Y ? ny : nz;
         const int idx = clampi(lo - 2 + i, -2, n + 2);
-        T* dst = axis == X ? TXs : axis == Y ? TYs : TZs;
+        T* dst = axis == X ? t.TXs : axis == Y ? t.TYs : t.TZs;
         cp_async_elem<sizeof(T)>(dst + k * len + i, g.tab[axis] + k * g.stride[axis] + idx + kTabOffset);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     // the control block's values, read while the copies are in flight
     const int failed = a.c->error;
-    const StageConst sc = stage_const(a.stage, a.c);
-    const T dt = (T)a.c->dt;
+    sc = stage_const(a.stage, a.c);
+    dt = (T)a.c->dt;
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    if (failed) return;
+    if (failed) return false;
     if (blend) {      // u of each impulse-box cell: the velocity box entry 2 cells further along its cross axes
         blend_box<T, MW, MH, G::MD, NT, UW, UP>(MX, SU, (2 * UH + 2) * UW, a.r, a.one_minus_r);
         blend_box<T, MW, MH, G::MD, NT, VW, VP>(MY, SV, 2 * VP + 2, a.r, a.one_minus_r);
         blend_box<T, MW, MH, G::MD, NT, WW, WP>(MZ, SW, 2 * WW + 2, a.r, a.one_minus_r);
         __syncthreads();
     }
-    const TabSlice<T, G::SX> tX{TXs, x0};
-    const TabSlice<T, G::SY> tY{TYs, y0};
-    const TabSlice<T, G::SZ> tZ{TZs, z0};
 
     // ---- K = u.m per cell (x0-1+ix, y0-1+iy, z0-1+iz)
     constexpr int KW = TX + 1, KRPS = NT / KW;
@@ -222,6 +229,29 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                           (w0[0] * MZ[mi] + w0[WP] * MZ[mi + MH * MW]));
     }
     __syncthreads();
+    return true;
+}
+
+template <class T, int TY, int TZ, int NT>
+__device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
+    using G = TileGeom<TY, TZ, NT>;
+    constexpr int TX = G::TX, RPT = G::ROWS_PER_THREAD;
+    constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
+    constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;      // plane strides of the velocity boxes
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const TileArrays<T> ta = tile_arrays<T, G>(smem_raw);
+    StageConst sc;
+    T dt;
+    if (!tile_prologue<T, TY, TZ, NT>(a, blk, ta, sc, dt)) return;
+    T *SU = ta.SU, *SV = ta.SV, *SW = ta.SW, *MX = ta.MX, *MY = ta.MY, *MZ = ta.MZ, *Kc = ta.Kc;
+    const Params& p = a.p;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int x0 = blk.x * TX, y0 = blk.y * TY, z0 = blk.z * TZ;
+    const int o4 = p.o4;
+    const bool blend = a.stage == 0;
+    const TabSlice<T, G::SX> tX{ta.TXs, x0};
+    const TabSlice<T, G::SY> tY{ta.TYs, y0};
+    const TabSlice<T, G::SZ> tZ{ta.TZs, z0};
 
     const T lidv = (T)lid_speed(p, sc.tau);
     const T half = T(0.5), eighth = T(0.125);
