@@ -238,7 +238,7 @@ def transforms_roofline(settings, ms_per_pass, tc, peak_gbs, launches=6):
     nbytes = (3 * 16 + 16 if paired else 6 * 16 + 8) * cells
     s = ms_per_pass / 1e3
     peak = gemm_peak_tflops('tf32' if tc else 'fp64')
-    name = ('tc_transform_kernel (3xTF32)' if tc else
+    name = ('tc2_transform_kernel / tc_transform_kernel (tcgen05 3xTF32)' if tc else
             'pair_xy/pair_z/pair_yx_kernel (FP64 DMMA, two transforms per launch)' if paired else
             'dgemm_mma_kernel (FP64 DMMA)')
     return {'kernel': name, 'launches_per_pass': launches,
