@@ -102,7 +102,8 @@ long long cavity_estimate_bytes(const CavityConfig* config, int precision);
 int cavity_time_steps(CavitySolver* s, int warmup, int steps, int flush_l2, float* ms_per_step, float* kernel_ms);
 /* Autotuner (no counterpart in the reference): times `steps` whole steps from the current state under each
  * candidate, restoring the state after each, and keeps the fastest for this cavity, in two rounds: the momentum
- * sweep (the tile kernel, or the z-march with 1/2, 1, 2 or 4 times its device-filling z-chunk count; only the
+ * sweep (the tile kernel, in FP32 also its packed two-cells-per-thread form, or the z-march with 1/2, 1, 2 or 4
+ * times its device-filling z-chunk count; only the
  * kernel CAVITY_SWEEP names, when set), then the FP64 transforms (six launches of 64 x 64 or 32 x 32 tiles, one
  * cooperative launch of 32 x 32 tiles, or, where no axis exceeds 64 cells, three launches of two chained
  * transforms each).  The choice is cached per grid size, stretching and precision form

@@ -29,7 +29,7 @@ namespace cavity {
 // launch (kind, template variant, grid, dynamic shared memory and argument record) to it instead of launching:
 // a batch of cavities collects every member's arguments for the same launch sequence this way and issues one
 // batched launch per entry.
-enum SweepKind : int { kSweepFace = 0, kSweepTile = 1, kSweepMarch = 2 };
+enum SweepKind : int { kSweepFace = 0, kSweepTile = 1, kSweepMarch = 2, kSweepPair = 3 };
 enum LaunchKind : int { kLkStepBegin = 0, kLkSweep, kLkStart, kLkResidual, kLkFinish, kLkDgemm64, kLkDgemm32, kLkTc,
                         kLkPair };
 struct LaunchRecord {

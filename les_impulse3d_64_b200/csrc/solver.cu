@@ -28,6 +28,7 @@
 #include "sweep.cuh"
 #include "sweep_march.cuh"
 #include "sweep_tile.cuh"
+#include "sweep_pair.cuh"
 #include "outputs.cuh"
 #include "setup.h"
 
@@ -192,6 +193,9 @@ template <class T> class Solver : public SolverBase {
     static constexpr int kTileTZ = 4;
     static constexpr int kTileNT = sizeof(T) == 8 ? 256 : 512;     // threads: registers allow 512 in FP32
     using TileG = TileGeom<kTileTY, kTileTZ, kTileNT>;
+    // the FP32 tile sweep with two cells per thread in packed arithmetic (sweep_pair.cuh): the same tile, 256 threads
+    static constexpr int kPairNT = 256;
+    using PairG = TileGeom<kTileTY, kTileTZ, kPairNT>;
     // the z-march sweep (sweep_march.cuh): 32 x 8 columns of cells per CTA
     static constexpr int kMarchTX = 32, kMarchTY = 8;
     using MarchG = MarchGeom<kMarchTX, kMarchTY>;
@@ -650,7 +654,8 @@ public:
 
     // Time whole steps under each candidate launch shape from the current state, restore the state after each,
     // and keep the fastest (cached per grid size, stretching and precision; see Tuning).  Two rounds: first the
-    // momentum sweep (the tile kernel, or the march with 1/2, 1, 2 and 4 times its device-filling z-chunk count;
+    // momentum sweep (the tile kernel, in FP32 also its packed two-cells-per-thread form, or the march with 1/2, 1,
+    // 2 and 4 times its device-filling z-chunk count;
     // only the chosen kernel when CAVITY_SWEEP names one), then, with the fastest sweep, the FP64 transforms where
     // they run (64 x 64 tiles, 32 x 32 tiles, 32 x 32 tiles in one cooperative launch, and three paired launches
     // where no axis exceeds 64 cells).
@@ -703,6 +708,7 @@ public:
         const int forced = sweep_forced_ ? sweep_kind_ : -1;
         std::vector<Tuning> sweeps;
         if (forced < 0 || forced == kSweepTile) sweeps.push_back(Tuning{0, 0, -1, kSweepTile, 0});
+        if (sizeof(T) == 4 && (forced < 0 || forced == kSweepPair)) sweeps.push_back(Tuning{0, 0, -1, kSweepPair, 0});
         if (forced < 0 || forced == kSweepMarch) {
             const int kind = sweep_kind_;
             sweep_kind_ = kSweepMarch;
@@ -994,6 +1000,13 @@ private:
             if (!record_launch(kLkSweep, kSweepMarch, grid, G::template smem_bytes<T>(), a))
                 check(launch_pdl(sweep_march_kernel<T, kMarchTX, kMarchTY>, grid, dim3(G::NT),
                                  G::template smem_bytes<T>(), st, a));
+        } else if (sweep_kind_ == kSweepPair) {
+            if constexpr (sizeof(T) == 4) {
+                const dim3 grid((nx_ + TileG::TX - 1) / TileG::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
+                const size_t smem = PairG::template smem_bytes<T>();
+                if (!record_launch(kLkSweep, kSweepPair, grid, smem, a))
+                    check(launch_pdl(sweep_pair_kernel<kTileTY, kTileTZ, kPairNT>, grid, dim3(kPairNT), smem, st, a));
+            }
         } else if (sweep_kind_ == kSweepTile) {
             using G = TileG;
             dim3 grid((nx_ + G::TX - 1) / G::TX, (ny_ + kTileTY - 1) / kTileTY, (nz_ + kTileTZ - 1) / kTileTZ);
@@ -1172,15 +1185,21 @@ private:
 
     void build_graphs() {
         {
-            // momentum sweep: shared-memory tiles unless CAVITY_SWEEP=march (the z-march, sweep_march.cuh) or =face
-            // (a thread per face).  The march evaluates each edge once but measured slower than the tiles (C2:
+            // momentum sweep: shared-memory tiles (FP32: two cells per thread, packed) unless CAVITY_SWEEP=march (the
+            // z-march, sweep_march.cuh), =face (a thread per face) or =tile (one cell per thread).  The march evaluates each edge once but measured slower than the tiles (C2:
             // 54.6 against 40.6 us per launch; 128^3 mixed: 196 against 133 us), so it is not the default.
             const char* sw = std::getenv("CAVITY_SWEEP");
             const std::string kind = sw ? sw : "";
             sweep_kind_ = kind == "face" ? kSweepFace : kind == "march" ? kSweepMarch : kSweepTile;
+            // the FP32 default is the packed two-cells-per-thread tile kernel (sweep_pair.cuh); CAVITY_SWEEP=tile
+            // selects one cell per thread
+            if (kind == "pair" || (kind.empty() && sizeof(T) == 4)) sweep_kind_ = sizeof(T) == 4 ? kSweepPair : kSweepTile;
             sweep_forced_ = !kind.empty();
             check(cudaFuncSetAttribute(sweep_tile_kernel<T, kTileTY, kTileTZ, kTileNT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TileG::template smem_bytes<T>()));
+            if constexpr (sizeof(T) == 4)
+                check(cudaFuncSetAttribute(sweep_pair_kernel<kTileTY, kTileTZ, kPairNT>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PairG::template smem_bytes<T>()));
             {
                 const int smem = (int)MarchG::template smem_bytes<T>();
                 check(cudaFuncSetAttribute(sweep_march_kernel<T, kMarchTX, kMarchTY>,
@@ -1389,6 +1408,9 @@ public:
         check(cudaFuncSetAttribute(sweep_march_batched<T, S_::kMarchTX, S_::kMarchTY>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)S_::MarchG::template smem_bytes<T>()));
+        if constexpr (sizeof(T) == 4)
+            check(cudaFuncSetAttribute(sweep_pair_batched<kTY, kTZ, S_::kPairNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)S_::PairG::template smem_bytes<T>()));
         if (f.tc_fdm_) check(tc_transform_prepare_batched());
         check(pair_prepare());
         for (int S = 0; S < 2; S++) build(S);
@@ -1612,7 +1634,11 @@ private:
             if (r.variant == kSweepMarch)
                 check(launch_pdl(sweep_march_batched<T, S_::kMarchTX, S_::kMarchTY>, g, dim3(S_::MarchG::NT), r.smem, st,
                                  (const MomentumArgs<T>*)d, items, live));
-            else
+            else if (r.variant == kSweepPair) {
+                if constexpr (sizeof(T) == 4)
+                    check(launch_pdl(sweep_pair_batched<kTY, kTZ, S_::kPairNT>, g, dim3(S_::kPairNT), r.smem, st,
+                                     (const MomentumArgs<T>*)d, items, live));
+            } else
                 check(launch_pdl(sweep_tile_batched<T, kTY, kTZ, kNT>, g, dim3(kNT), r.smem, st,
                                  (const MomentumArgs<T>*)d, items, live));
             break;

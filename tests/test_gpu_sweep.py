@@ -67,3 +67,47 @@ def test_march_chunks_do_not_change_the_step(chunks):
     _, f = run(s, 'fp64', {'CAVITY_SWEEP': 'march', 'CAVITY_MARCH_CHUNKS': chunks})
     for k in FIELDS:
         assert np.array_equal(f[k], ref[k]), k
+
+
+@pytest.mark.parametrize('grid', range(len(GRIDS)))
+def test_packed_pair_sweep_matches_tile_sweep(grid):
+    """The FP32 sweep with two cells per thread in packed FP32x2 arithmetic (CAVITY_SWEEP=pair, sweep_pair.cuh)
+    against the one-cell-per-thread tile kernel: the same expressions and sums, so the mixed form's fields agree
+    to FP32 rounding."""
+    s = base_settings(adaptive_dt=1, dt_max=0.01, nu=0.002, **GRIDS[grid])
+    rp, fp = run(s, 'mixed', {'CAVITY_SWEEP': 'pair'})
+    rt, ft = run(s, 'mixed', {'CAVITY_SWEEP': 'tile'})
+    for a, b in zip(rp, rt):
+        assert a['dt_reason'] == b['dt_reason'] and a['phi_passes'] == b['phi_passes']
+    for k in FIELDS:
+        err = float(np.abs(fp[k] - ft[k]).max() / max(np.abs(ft[k]).max(), 1e-30))
+        assert err <= 2e-6, (k, err)
+
+
+def test_packed_pair_sweep_in_a_batch():
+    """A mixed-form batch of cavities of three sizes with the packed FP32x2 sweep equals the same batch with the
+    tile sweep to FP32 rounding."""
+    from les_impulse3d_64_b200 import workloads
+    from les_impulse3d_64_b200.ensemble import Ensemble
+    cases = workloads.ensemble_cases(count=6, seed=13, sizes=(16, 24, 40), re_range=(100.0, 2000.0))
+    out = {}
+    for kind in ('pair', 'tile'):
+        old = os.environ.get('CAVITY_SWEEP')
+        os.environ['CAVITY_SWEEP'] = kind
+        try:
+            ens = Ensemble(cases, group='precision')
+        finally:
+            if old is None:
+                os.environ.pop('CAVITY_SWEEP', None)
+            else:
+                os.environ['CAVITY_SWEEP'] = old
+        try:
+            ens.advance(3, chunk=3)
+            out[kind] = [ens.fields(i) for i in range(len(cases))]
+        finally:
+            ens.close()
+    for i in range(len(cases)):
+        for k in out['tile'][i]:
+            a, b = out['pair'][i][k], out['tile'][i][k]
+            err = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+            assert err <= 2e-6, (i, k, err)
