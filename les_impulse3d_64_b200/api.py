@@ -306,7 +306,8 @@ class Cavity:
 
     def autotune(self, steps=6):
         """Pick the fastest launch shapes for this cavity by timing `steps` steps per candidate (state restored);
-        returns (march z-chunks, FP64 transform tile, one-launch pass, ms per step).  See cavity_autotune."""
+        returns (march z-chunks, FP64 transform tile, FP64 pass form (0 six launches, 1 one cooperative launch,
+        2 three paired launches, -1 the size rule), ms per step).  See cavity_autotune."""
         L = self.lib
         L.cavity_autotune.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]
         chunks, tile, fused, ms = ct.c_int(0), ct.c_int(0), ct.c_int(0), ct.c_float(0)
