@@ -71,6 +71,16 @@ def load_library(library=None):
     return lib
 
 
+def _field_buffer(shape, name, out):
+    """`out`, checked, or a new array for a field: float64 for phi, float32 for the others (python_api.py)."""
+    dtype = np.float64 if name == 'phi' else np.float32
+    if out is None:
+        return np.empty(shape, dtype=dtype)
+    if out.shape != tuple(shape) or out.dtype != dtype or not out.flags['C_CONTIGUOUS']:
+        raise ValueError(f'{name}: output buffer must be C-contiguous {dtype.__name__} of shape {tuple(shape)}')
+    return out
+
+
 def make_config(settings):
     """Config record from a settings dict, copying fields by name; `probes` is a list of (x/L, y/L)."""
     config = Config()
@@ -143,8 +153,10 @@ class Solver:
         self.call('solver_diagnostics', ct.byref(d))
         return {name: getattr(d, name) for name, _ in Diagnostics._fields_}
 
-    def field(self, name):
-        out = np.empty(self.shapes[name], dtype=np.float64 if name == 'phi' else np.float32)
+    def field(self, name, out=None):
+        """A field as python_api returns it; `out` (an addition): a C-contiguous array of the field's shape and
+        dtype to copy into, so that a caller reading fields repeatedly reuses its buffers."""
+        out = _field_buffer(self.shapes[name], name, out)
         self.call('solver_get_field', FIELD_NUMBER[name], pointer(out))
         return out
 
@@ -262,8 +274,8 @@ class Cavity:
         self._call('cavity_sync', self.handle, ct.byref(r))
         return Solver._as_dict(r)
 
-    def field(self, name):
-        out = np.empty(self.shapes[name], dtype=np.float64 if name == 'phi' else np.float32)
+    def field(self, name, out=None):
+        out = _field_buffer(self.shapes[name], name, out)
         self._call('cavity_get_field', self.handle, FIELD_NUMBER[name], pointer(out))
         return out
 

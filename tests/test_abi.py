@@ -60,3 +60,16 @@ def test_calls_without_solver_fail_with_message(lib):
     assert lib.solver_report(ct.byref(r)) == 1
     assert lib.solver_last_error() == b'no solver: call solver_create first'
     assert lib.solver_destroy() == 0
+
+
+def test_field_output_buffer_is_checked():
+    """`field(name, out=...)` copies into a caller's buffer only when it has the field's shape and dtype."""
+    import numpy as np
+    from les_impulse3d_64_b200.api import _field_buffer
+    a = np.zeros((4, 3, 5), dtype=np.float32)
+    assert _field_buffer((4, 3, 5), 'u', a) is a
+    assert _field_buffer((4, 3, 5), 'phi', None).dtype == np.float64
+    for bad in (np.zeros((4, 3, 5), dtype=np.float64), np.zeros((4, 3, 6), dtype=np.float32),
+                np.zeros((4, 5, 3), dtype=np.float32).transpose(0, 2, 1)):
+        with pytest.raises(ValueError):
+            _field_buffer((4, 3, 5), 'u', bad)
