@@ -102,3 +102,30 @@ def test_batch_pass_forms_agree(form):
     for i in range(len(cases)):
         for k in ref[i]:
             assert np.array_equal(ref[i][k], got[i][k]), (i, k)
+
+
+def test_batch_with_an_axis_beyond_the_paired_pass():
+    """A batch whose members include one with 80 cells per axis runs every member's FP64 passes as six launches
+    (the paired pass takes at most 64 per axis, and a batch's members share their launches); each member ends equal
+    to itself alone, which runs the paired pass when it fits, to rounding."""
+    cases = workloads.ensemble_cases(count=3, seed=17, sizes=(24, 80), re_range=(100.0, 2000.0))
+    cases[0]['settings'] = workloads.settings(80, 500.0, beta=1.5, cfl=0.5)
+    for c in cases:
+        c['precision'] = 'fp64'
+    ens = Ensemble(cases, group='precision')
+    try:
+        assert len(ens.batches) == 1
+        ens.advance(3, chunk=3)
+        together = [ens.fields(i) for i in range(len(cases))]
+    finally:
+        ens.close()
+    for i in range(len(cases)):
+        alone = Ensemble([cases[i]], batched=False)
+        try:
+            alone.advance(3, chunk=1)
+            f = alone.fields(0)
+        finally:
+            alone.close()
+        for k in f:
+            err = float(np.abs(f[k] - together[i][k]).max() / max(np.abs(f[k]).max(), 1e-30))
+            assert err <= 1e-10, (i, k, err)
