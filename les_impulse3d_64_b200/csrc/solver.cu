@@ -1006,6 +1006,8 @@ private:
                 const size_t smem = PairG::template smem_bytes<T>();
                 if (!record_launch(kLkSweep, kSweepPair, grid, smem, a))
                     check(launch_pdl(sweep_pair_kernel<kTileTY, kTileTZ, kPairNT>, grid, dim3(kPairNT), smem, st, a));
+            } else {
+                fail("the packed sweep is FP32 only");
             }
         } else if (sweep_kind_ == kSweepTile) {
             using G = TileG;
@@ -1638,6 +1640,8 @@ private:
                 if constexpr (sizeof(T) == 4)
                     check(launch_pdl(sweep_pair_batched<kTY, kTZ, S_::kPairNT>, g, dim3(S_::kPairNT), r.smem, st,
                                      (const MomentumArgs<T>*)d, items, live));
+                else
+                    fail("the packed sweep is FP32 only");
             } else
                 check(launch_pdl(sweep_tile_batched<T, kTY, kTZ, kNT>, g, dim3(kNT), r.smem, st,
                                  (const MomentumArgs<T>*)d, items, live));
