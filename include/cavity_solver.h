@@ -168,6 +168,13 @@ int cavity_batch_create(CavitySolver* const* members, int count, CavityBatch** o
 int cavity_batch_create_slots(CavitySolver* const* members, int count, int capacity, CavityBatch** out);
 int cavity_batch_set_member(CavityBatch* b, int slot, CavitySolver* s);
 int cavity_batch_size(const CavityBatch* b);
+/* Advances the batch `steps` steps through an instrumented copy of its step graph (built from the current members)
+ * and fills ms[4] with the mean device time per step, in milliseconds summed over the three stages, of: the
+ * momentum sweeps; the projection starts with the residuals of their warm-start guesses; each stage's first
+ * pressure pass (transforms and residual; further passes, inside the refinement loop, are not timed); and the
+ * finishes.  The steps are ordinary steps (the same kernels in the same order); no steps may be queued.  No
+ * counterpart in the reference. */
+int cavity_batch_part_times(CavityBatch* b, int steps, double* ms);
 int cavity_batch_step_async(CavityBatch* b, int count);
 int cavity_batch_sync(CavityBatch* b, CavityReport* reports);
 int cavity_batch_destroy(CavityBatch* b);

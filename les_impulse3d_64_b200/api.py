@@ -417,6 +417,7 @@ class Batch:
         L.cavity_batch_step_async.argtypes = [ct.c_void_p, ct.c_int]
         L.cavity_batch_sync.argtypes = [ct.c_void_p, ct.c_void_p]
         L.cavity_batch_destroy.argtypes = [ct.c_void_p]
+        L.cavity_batch_part_times.argtypes = [ct.c_void_p, ct.c_int, ct.c_void_p]
         handles = (ct.c_void_p * len(cavities))(*[c.handle.value for c in cavities])
         self.handle = ct.c_void_p()
         self._call('cavity_batch_create_slots', handles, len(cavities), capacity, ct.byref(self.handle))
@@ -439,6 +440,14 @@ class Batch:
 
     def step_async(self, count=1):
         self._call('cavity_batch_step_async', self.handle, int(count))
+
+    def part_times(self, steps=4):
+        """Mean device time per step (ms, three stages) of the sweeps, the projection starts with their guesses'
+        residuals, the first pressure pass of each stage and the finishes, over `steps` ordinary steps through an
+        instrumented graph (cavity_batch_part_times)."""
+        ms = (ct.c_double * 4)()
+        self._call('cavity_batch_part_times', self.handle, int(steps), ms)
+        return dict(zip(('sweep', 'start', 'first_pass', 'finish'), list(ms)))
 
     def sync(self):
         """Wait for the queued steps; the report of every slot (None for an empty slot)."""

@@ -1358,6 +1358,7 @@ public:
     virtual void sync(CavityReport* reports) = 0;
     virtual int size() const = 0;
     virtual void set_member(int slot, SolverBase* s) = 0;
+    virtual void part_times(int steps, double* ms) = 0;
 };
 
 template <class T> class Batch : public BatchBase {
@@ -1425,17 +1426,58 @@ public:
             if (graph_[S]) cudaGraphDestroy(graph_[S]);
             if (dargs_[S]) cudaFree(dargs_[S]);
         }
+        drop_timing();
+        for (cudaEvent_t& e : tev_)
+            if (e) cudaEventDestroy(e);
         if (stream_) cudaStreamDestroy(stream_);
         if (body_stream_) cudaStreamDestroy(body_stream_);
     }
     int size() const override { return (int)m_.size(); }
 
     void step_async(int count) override {
-        for (int i = 0; i < count; i++) {
+        for (int i = 0; i < count; i++) launch_step(exec_);
+    }
+    // Per-step device time (ms, summed over the three stages) of the batch's parts: the sweeps, the projection
+    // starts with the residuals of their guesses, the first pressure pass of each stage (transforms and
+    // residual), and the finishes, over `steps` steps through a second graph with events between the parts.
+    // The steps advance the cavities as cavity_batch_step_async does (the same kernels in the same order).
+    void part_times(int steps, double* ms) override {
+        if (queued_) fail("batch: steps are queued; sync first");
+        if (!tev_[0])
+            for (cudaEvent_t& e : tev_) check(cudaEventCreate(&e));
+        drop_timing();
+        for (int S = 0; S < 2; S++) build(S, true);
+        for (int k = 0; k < kParts; k++) ms[k] = 0;
+        for (int i = 0; i < steps; i++) {
+            launch_step(texec_);
+            sync(nullptr);
+            for (int stage = 0; stage < 3; stage++)
+                for (int k = 0; k < kParts; k++) {
+                    float t = 0;
+                    check(cudaEventElapsedTime(&t, tev_[(stage * kParts + k) * 2], tev_[(stage * kParts + k) * 2 + 1]));
+                    ms[k] += t / std::max(steps, 1);
+                }
+        }
+    }
+    static constexpr int kParts = 4;
+
+private:
+    void drop_timing() {
+        for (int S = 0; S < 2; S++) {
+            if (texec_[S]) cudaGraphExecDestroy(texec_[S]);
+            if (tgraph_[S]) cudaGraphDestroy(tgraph_[S]);
+            if (targs_[S]) cudaFree(targs_[S]);
+            texec_[S] = nullptr;
+            tgraph_[S] = nullptr;
+            targs_[S] = nullptr;
+        }
+    }
+    void launch_step(cudaGraphExec_t* exec) {
+        {
             for (size_t k = 0; k < m_.size(); k++)
                 if (m_[k] && m_[k]->par_ != (par_ ^ d_[k]))
                     fail("batch: the cavities' states have diverged (a failed step); rebuild the batch");
-            check(cudaGraphLaunch(exec_[par_], stream_));
+            check(cudaGraphLaunch(exec[par_], stream_));
             for (S_* s : m_) {
                 if (!s) continue;
                 if (s->pending_.empty()) s->steps_before_ = s->hc_.steps;
@@ -1448,6 +1490,8 @@ public:
             queued_ = true;
         }
     }
+
+public:
     // waits for the queued steps; every occupied slot's report (its last good state if it failed; an empty
     // slot's report is zero with steps = -1), then the first failure as an error naming the slot
     void sync(CavityReport* reports) override {
@@ -1671,14 +1715,21 @@ private:
     // the step of batch parity S (as Solver::enqueue_step, each slot at its own state parity S ^ d); `launch` =
     // false only records (sizes the argument buffer), true captures the batched launches into the graph being
     // built on stream_
-    void sequence(int S, std::vector<unsigned char>& host, Layout& L, bool launch) {
+    void sequence(int S, std::vector<unsigned char>& host, Layout& L, bool launch, bool timing = false) {
+        // timing: events before and after the parts of each stage outside the refinement loop (part_times)
+        auto mark = [&](int stage, int part, int end) {
+            if (timing && launch)
+                check(cudaEventRecordWithFlags(tev_[(stage * kParts + part) * 2 + end], stream_, cudaEventRecordExternal));
+        };
         L.live = 0;
         host.resize(align256(sizeof(int) * m_.size()));
         for (size_t i = 0; i < m_.size(); i++) reinterpret_cast<int*>(host.data())[i] = m_[i] ? 1 : 0;
         auto par = [&](int b) { return S ^ d_[b]; };
         emit(stream_, [&](S_& s, int) { s.launch_step_begin(stream_); }, host, L, launch);
         for (int stage = 0; stage < 3; stage++) {
+            mark(stage, 0, 0);
             emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 0); }, host, L, launch);
+            mark(stage, 0, 1);
             cudaGraph_t g = nullptr;
             const cudaGraphNode_t* deps = nullptr;
             size_t ndeps = 0;
@@ -1687,9 +1738,13 @@ private:
                 check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
                 check(cudaGraphConditionalHandleCreate(&handles_[S][stage], g, 0, cudaGraphCondAssignDefault));
             }
+            mark(stage, 1, 0);
             emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 1); }, host, L, launch);
+            mark(stage, 1, 1);
             // the first pass outside the loop (see Solver::captured_loop), then the loop
+            mark(stage, 2, 0);
             emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 2); }, host, L, launch);
+            mark(stage, 2, 1);
             if (launch) {
                 check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &g, &deps, &ndeps));
                 cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
@@ -1707,10 +1762,34 @@ private:
             } else {
                 emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 3); }, host, L, launch);
             }
+            mark(stage, 3, 0);
             emit(stream_, [&](S_& s, int b) { member_part(s, par(b), S, stage, 4); }, host, L, launch);
+            mark(stage, 3, 1);
         }
     }
-    void build(int S) {
+    // the step graph of batch parity S; with `timing` the instrumented twin (part_times), built from the current
+    // members with its own argument buffer and refinement-loop handles (the plain graph's are kept)
+    void build(int S, bool timing = false) {
+        if (timing) {
+            cudaGraphConditionalHandle saved[3] = {handles_[S][0], handles_[S][1], handles_[S][2]};
+            std::vector<unsigned char> host;
+            Layout L;
+            item_lists_.clear();
+            sequence(S, host, L, false);
+            check(cudaMalloc(&targs_[S], std::max<size_t>(host.size(), 256)));
+            dargs_cur_ = targs_[S];
+            host.clear();
+            item_lists_.clear();
+            L = Layout();
+            check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            sequence(S, host, L, true, true);
+            check(cudaStreamEndCapture(stream_, &tgraph_[S]));
+            check(cudaGraphInstantiate(&texec_[S], tgraph_[S], 0));
+            check(cudaMemcpy(targs_[S], host.data(), host.size(), cudaMemcpyHostToDevice));
+            for (int k = 0; k < 3; k++) handles_[S][k] = saved[k];
+            dargs_cur_ = dargs_[S];
+            return;
+        }
         std::vector<unsigned char> host;
         Layout L;
         item_lists_.clear();
@@ -1736,8 +1815,10 @@ private:
     int nx_ = 0, ny_ = 0, nz_ = 0, sweep_kind_ = 0;
     bool tc_fdm_ = false;
     cudaStream_t stream_ = nullptr, body_stream_ = nullptr;
-    cudaGraph_t graph_[2] = {nullptr, nullptr};
-    cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+    cudaGraph_t graph_[2] = {nullptr, nullptr}, tgraph_[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec_[2] = {nullptr, nullptr}, texec_[2] = {nullptr, nullptr};
+    cudaEvent_t tev_[3 * kParts * 2] = {};
+    void* targs_[2] = {nullptr, nullptr};     // argument buffers of the timing graphs
     cudaGraphConditionalHandle handles_[2][3] = {};
     void* dargs_[2] = {nullptr, nullptr};
     void* dargs_cur_ = nullptr;
@@ -2118,6 +2199,12 @@ int cavity_batch_set_member(CavityBatch* b, int slot, CavitySolver* s) {
     });
 }
 int cavity_batch_size(const CavityBatch* b) { return b && b->b ? b->b->size() : -1; }
+int cavity_batch_part_times(CavityBatch* b, int steps, double* ms) {
+    return safely([&] {
+        if (!b || !b->b || !ms || steps < 1) cavity::fail("batch part times: null batch or output, or steps < 1");
+        b->b->part_times(steps, ms);
+    });
+}
 int cavity_batch_destroy(CavityBatch* b) { return safely([&] { delete b; }); }
 const char* cavity_last_error(void) { return g_last_error.c_str(); }
 }

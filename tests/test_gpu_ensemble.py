@@ -129,3 +129,25 @@ def test_batch_with_an_axis_beyond_the_paired_pass():
         for k in f:
             err = float(np.abs(f[k] - together[i][k]).max() / max(np.abs(f[k]).max(), 1e-30))
             assert err <= 1e-10, (i, k, err)
+
+
+def test_batch_part_times_are_ordinary_steps():
+    """cavity_batch_part_times times a batch's parts (sweep, start with the guess residual, first pass, finish)
+    through an instrumented copy of its graph: every part takes time, the steps it takes leave the cavities bit for
+    bit where plain batched steps leave them, and the plain graph steps on correctly afterwards."""
+    cases = workloads.ensemble_cases(count=4, seed=19, sizes=(16, 24), re_range=(100.0, 2000.0))
+    ens_a, ens_b = Ensemble(cases, group='precision'), Ensemble(cases, group='precision')
+    try:
+        assert len(ens_a.batches) == 1
+        times = ens_a.batches[0].part_times(3)
+        assert set(times) == {'sweep', 'start', 'first_pass', 'finish'} and all(t > 0 for t in times.values())
+        ens_b.advance(3, chunk=3)
+        for e in (ens_a, ens_b):
+            e.advance(2, chunk=2)
+        for i in range(len(cases)):
+            fa, fb = ens_a.fields(i), ens_b.fields(i)
+            for k in fa:
+                assert np.array_equal(fa[k], fb[k]), (i, k)
+    finally:
+        ens_a.close()
+        ens_b.close()
