@@ -129,9 +129,17 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
     auto w3 = [&](F2 lA, T lB) { return -((lA * f2(lB)) * f2(eighth)); };
     auto w3s = [&](T lA, F2 lB) { return -((f2(lA) * lB) * f2(eighth)); };
 
+    // A half-warp takes RPT consecutive rows of one column of the tile, and the corner edges of each cell are
+    // evaluated once for the two faces each feeds, the y- and x-edges on z-face z + 1 carrying over to the next
+    // row, as in the tile kernel (sweep_tile_body); the terms are the same packed expressions as before.
+    constexpr int RPT = TY * TZ / PAIR_ROWS;
+    static_assert(PAIR_ROWS % TY == 0 && PAIR_ROWS / TY * RPT == TZ, "a half-warp's rows are one column of the tile");
+    const int hw = 2 * warp + (lane >> 4);
+    F2 cyWo = f2(0.f), cyU = f2(0.f), cyUl = f2(0.f), cyUh = f2(0.f);    // y-edge (x, z + 1)
+    F2 cxWo = f2(0.f), cxV = f2(0.f), cxVl = f2(0.f), cxVh = f2(0.f);    // x-edge (y, z + 1)
 #pragma unroll 1
-    for (int r = 0; r < TY * TZ / PAIR_ROWS; r++) {
-        const int row = 2 * warp + (lane >> 4) + PAIR_ROWS * r, ry = row % TY, rz = row / TY;
+    for (int r = 0; r < RPT; r++) {
+        const int ry = hw % TY, rz = RPT * (hw / TY) + r;
         const int x = x0 + px, y = y0 + ry, z = z0 + rz;
         if (x >= nx || y >= ny || z >= nz) continue;
         const bool vb = x + 1 < nx;                           // the pair's second cell is inside
@@ -147,15 +155,65 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
         const F2 bv = rk ? f2(__ldg(a.m0[Y] + iv), vb ? __ldg(a.m0[Y] + iv + 1) : 0.f) : zero;
         const F2 bw = rk ? f2(__ldg(a.m0[Z] + iw), vb ? __ldg(a.m0[Z] + iw + 1) : 0.f) : zero;
         auto store = [&](T* out, int i, F2 v, bool zero_a) {
-            out[i] = zero_a ? T(0) : v.v.x;
-            if (vb) out[i + 1] = v.v.y;
+            st_out(out + i, zero_a ? T(0) : v.v.x);
+            if (vb) st_out(out + i + 1, v.v.y);
         };
+
+        // ---------------- the corner edges: narrow terms of two faces each
+        F2 uZ0, vZ0, uY0, wY0, vX0, wX0, uY1, vX1;
+        {
+            const F2 ok1x = tx2(kOk1, x), l1x = tx2(kL1, x), i1x = tx2(kInvSp, x), e1lx = tx2(kEv1Lo, x),
+                     e1hx = tx2(kEv1Hi, x);
+            const T ok1y = tY(kOk1, y), l1y = tY(kL1, y), i1y = tY(kInvSp, y);
+            const F2 e1ly = f2(tY(kEv1Lo, y)), e1hy = f2(tY(kEv1Hi, y)), e1lz = f2(tZ(kEv1Lo, z)), e1hz = f2(tZ(kEv1Hi, z));
+            {   // z-edge (x, y)
+                const F2 vl = ld2(pv - 1), vh = ld2(pv), ul = ld2(pu - UW), uh = ld2(pu);
+                const F2 wo = w1(ok1x, ok1y, l1x, l1y) * fms2(vh - vl, i1x, uh - ul, f2(i1y));
+                uZ0 = wo * fma2(e1lx, vl, e1hx * vh);
+                vZ0 = -(wo * fma2(e1ly, ul, e1hy * uh));
+            }
+            if (r == 0) {
+                const T ok1z = tZ(kOk1, z), l1z = tZ(kL1, z), i1z = tZ(kInvSp, z);
+                {   // y-edge (x, z)
+                    const F2 ul = ld2(pu - UP), uh = ld2(pu), wl = ld2(pw - 1), wh = ld2(pw);
+                    const F2 wo = w1s(ok1z, ok1x, l1z, l1x) * fms2(uh - ul, f2(i1z), wh - wl, i1x);
+                    uY0 = -(wo * fma2(e1lx, wl, e1hx * wh));
+                    wY0 = wo * fma2(e1lz, ul, e1hz * uh);
+                }
+                {   // x-edge (y, z)
+                    const F2 wl = ld2(pw - WW), wh = ld2(pw), vl = ld2(pv - VP), vh = ld2(pv);
+                    const F2 wo = f2(w1v(o4, ok1y, ok1z, l1y, l1z, eighth)) * fms2(wh - wl, f2(i1y), vh - vl, f2(i1z));
+                    vX0 = wo * fma2(e1ly, wl, e1hy * wh);
+                    wX0 = -(wo * fma2(e1lz, vl, e1hz * vh));
+                }
+            } else {     // the previous row's edges on this cell's lower z-face
+                uY0 = cyU;
+                wY0 = cyWo * fma2(e1lz, cyUl, e1hz * cyUh);
+                vX0 = cxV;
+                wX0 = -(cxWo * fma2(e1lz, cxVl, e1hz * cxVh));
+            }
+            {   // the edges on z-face z + 1 (the next row's corner edges)
+                const T ok1 = tZ(kOk1, z + 1), l1 = tZ(kL1, z + 1), i1 = tZ(kInvSp, z + 1);
+                const F2 ul = ld2(pu), uh = ld2(pu + UP), wl = ld2(pw + WP - 1), wh = ld2(pw + WP);
+                cyWo = w1s(ok1, ok1x, l1, l1x) * fms2(uh - ul, f2(i1), wh - wl, i1x);
+                cyU = -(cyWo * fma2(e1lx, wl, e1hx * wh));
+                cyUl = ul;
+                cyUh = uh;
+                const F2 wl2 = ld2(pw + WP - WW), wh2 = ld2(pw + WP), vl = ld2(pv), vh = ld2(pv + VP);
+                cxWo = f2(w1v(o4, ok1y, ok1, l1y, l1, eighth)) * fms2(wh2 - wl2, f2(i1y), vh - vl, f2(i1));
+                cxV = cxWo * fma2(e1ly, wl2, e1hy * wh2);
+                cxVl = vl;
+                cxVh = vh;
+            }
+            uY1 = cyU;
+            vX1 = cxV;
+        }
 
         // ---------------- u-faces x, x + 1: z-edges (omega_z) and y-edges (omega_y)
         {
             if (blend) {
-                a.m0_out[X][iu] = MX[mo];
-                if (vb) a.m0_out[X][iu + 1] = MX[mo + 1];
+                st_out(a.m0_out[X] + (iu), MX[mo]);
+                if (vb) st_out(a.m0_out[X] + (iu + 1), MX[mo + 1]);
             }
             const F2 ok1x = tx2(kOk1, x), l1x = tx2(kL1, x), l3x = tx2(kL3, x), i1x = tx2(kInvSp, x),
                      i3x = tx2(kInvNd3, x);
@@ -173,12 +231,6 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
                 const F2 wo = w3(l3x, tY(kL3, e)) * fms2(vh - vl, i3x, uh - ul, f2(tY(kInvNd3, e)));
                 return wo * fma2(e3l, vl, e3h * vh);
             };
-            auto py1 = [&](int d) {
-                const int e = z + d;
-                const F2 ul = ld2(pu + (d - 1) * UP), uh = ld2(pu + d * UP), wl = ld2(pw + d * WP - 1), wh = ld2(pw + d * WP);
-                const F2 wo = w1s(tZ(kOk1, e), ok1x, tZ(kL1, e), l1x) * fms2(uh - ul, f2(tZ(kInvSp, e)), wh - wl, i1x);
-                return -(wo * fma2(e1l, wl, e1h * wh));
-            };
             auto py3 = [&](int d) {
                 const int e = z + d;
                 const F2 ul = ld2(pu + (d - 2) * UP), uh = ld2(pu + (d + 1) * UP), wl = ld2(pw + d * WP - 2),
@@ -186,7 +238,7 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
                 const F2 wo = w3s(tZ(kL3, e), l3x) * fms2(uh - ul, f2(tZ(kInvNd3, e)), wh - wl, i3x);
                 return -(wo * fma2(e3l, wl, e3h * wh));
             };
-            F2 L = fma2(half, pz1(1) + pz1(0), half * (py1(1) + py1(0)));
+            F2 L = fma2(half, pz1(1) + uZ0, half * (uY1 + uY0));
             if (o4) {
                 const F2 c3 = tx2(kC3, x);
                 L = fma2(c3, pz3(2) + pz3(-1), L);
@@ -197,19 +249,19 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
             store(a.out[X], iu, val, x == 0);
             const int xl = x + 1 == nx - 1 ? x + 1 : x == nx - 1 ? x : -1;     // the cell whose upper wall face is zero
             if (xl >= 0) {
-                if (blend) a.m0_out[X][iu + (xl - x) + 1] = MX[mo + (xl - x) + 1];
-                a.out[X][iu + (xl - x) + 1] = T(0);
+                if (blend) st_out(a.m0_out[X] + (iu + (xl - x) + 1), MX[mo + (xl - x) + 1]);
+                st_out(a.out[X] + (iu + (xl - x) + 1), T(0));
             }
         }
         // ---------------- v-faces y: z-edges (omega_z) and x-edges (omega_x)
         {
             if (blend) {
-                a.m0_out[Y][iv] = MY[mo];
-                if (vb) a.m0_out[Y][iv + 1] = MY[mo + 1];
+                st_out(a.m0_out[Y] + (iv), MY[mo]);
+                if (vb) st_out(a.m0_out[Y] + (iv + 1), MY[mo + 1]);
             }
             if (y == 0) {
-                a.out[Y][iv] = T(0);
-                if (vb) a.out[Y][iv + 1] = T(0);
+                st_out(a.out[Y] + (iv), T(0));
+                if (vb) st_out(a.out[Y] + (iv + 1), T(0));
             } else {
                 const T ok1y = tY(kOk1, y), l1y = tY(kL1, y), l3y = tY(kL3, y), i1y = tY(kInvSp, y), i3y = tY(kInvNd3, y);
                 const F2 e1l = f2(tY(kEv1Lo, y)), e1h = f2(tY(kEv1Hi, y)), e3l = f2(tY(kEv3Lo, y)), e3h = f2(tY(kEv3Hi, y));
@@ -225,13 +277,6 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
                     const F2 wo = w3(tx2(kL3, e), l3y) * fms2(vh - vl, tx2(kInvNd3, e), uh - ul, f2(i3y));
                     return -(wo * fma2(e3l, ul, e3h * uh));
                 };
-                auto px1 = [&](int d) {
-                    const int e = z + d;
-                    const F2 wl = ld2(pw + d * WP - WW), wh = ld2(pw + d * WP), vl = ld2(pv + (d - 1) * VP), vh = ld2(pv + d * VP);
-                    const F2 wo = f2(w1v(o4, ok1y, tZ(kOk1, e), l1y, tZ(kL1, e), eighth)) *
-                                  fms2(wh - wl, f2(i1y), vh - vl, f2(tZ(kInvSp, e)));
-                    return wo * fma2(e1l, wl, e1h * wh);
-                };
                 auto px3 = [&](int d) {
                     const int e = z + d;
                     const F2 wl = ld2(pw + d * WP - 2 * WW), wh = ld2(pw + d * WP + WW), vl = ld2(pv + (d - 2) * VP),
@@ -239,7 +284,7 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
                     const F2 wo = f2(-((l3y * tZ(kL3, e)) * eighth)) * fms2(wh - wl, f2(i3y), vh - vl, f2(tZ(kInvNd3, e)));
                     return wo * fma2(e3l, wl, e3h * wh);
                 };
-                F2 L = fma2(half, pz1(1) + pz1(0), half * (px1(1) + px1(0)));
+                F2 L = fma2(half, pz1(1) + vZ0, half * (vX1 + vX0));
                 if (o4) {
                     const F2 c3 = f2(tY(kC3, y));
                     L = fma2(c3, pz3(2) + pz3(-1), L);
@@ -251,22 +296,22 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
             }
             if (y == ny - 1) {
                 if (blend) {
-                    a.m0_out[Y][iv + nx] = MY[mo + MW];
-                    if (vb) a.m0_out[Y][iv + nx + 1] = MY[mo + MW + 1];
+                    st_out(a.m0_out[Y] + (iv + nx), MY[mo + MW]);
+                    if (vb) st_out(a.m0_out[Y] + (iv + nx + 1), MY[mo + MW + 1]);
                 }
-                a.out[Y][iv + nx] = T(0);
-                if (vb) a.out[Y][iv + nx + 1] = T(0);
+                st_out(a.out[Y] + (iv + nx), T(0));
+                if (vb) st_out(a.out[Y] + (iv + nx + 1), T(0));
             }
         }
         // ---------------- w-faces z: x-edges (omega_x) and y-edges (omega_y)
         {
             if (blend) {
-                a.m0_out[Z][iw] = MZ[mo];
-                if (vb) a.m0_out[Z][iw + 1] = MZ[mo + 1];
+                st_out(a.m0_out[Z] + (iw), MZ[mo]);
+                if (vb) st_out(a.m0_out[Z] + (iw + 1), MZ[mo + 1]);
             }
             if (z == 0) {
-                a.out[Z][iw] = T(0);
-                if (vb) a.out[Z][iw + 1] = T(0);
+                st_out(a.out[Z] + (iw), T(0));
+                if (vb) st_out(a.out[Z] + (iw + 1), T(0));
             } else {
                 const T ok1z = tZ(kOk1, z), l1z = tZ(kL1, z), l3z = tZ(kL3, z), i1z = tZ(kInvSp, z), i3z = tZ(kInvNd3, z);
                 const F2 e1l = f2(tZ(kEv1Lo, z)), e1h = f2(tZ(kEv1Hi, z)), e3l = f2(tZ(kEv3Lo, z)), e3h = f2(tZ(kEv3Hi, z));
@@ -296,7 +341,7 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
                     const F2 wo = w3s(l3z, tx2(kL3, e)) * fms2(uh - ul, f2(i3z), wh - wl, tx2(kInvNd3, e));
                     return wo * fma2(e3l, ul, e3h * uh);
                 };
-                F2 L = fma2(half, px1(1) + px1(0), half * (py1(1) + py1(0)));
+                F2 L = fma2(half, px1(1) + wX0, half * (py1(1) + wY0));
                 if (o4) {
                     const F2 c3 = f2(tZ(kC3, z));
                     L = fma2(c3, px3(2) + px3(-1), L);
@@ -308,11 +353,11 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
             }
             if (z == nz - 1) {
                 if (blend) {
-                    a.m0_out[Z][iw + nx * ny] = MZ[mo + MW * MH];
-                    if (vb) a.m0_out[Z][iw + nx * ny + 1] = MZ[mo + MW * MH + 1];
+                    st_out(a.m0_out[Z] + (iw + nx * ny), MZ[mo + MW * MH]);
+                    if (vb) st_out(a.m0_out[Z] + (iw + nx * ny + 1), MZ[mo + MW * MH + 1]);
                 }
-                a.out[Z][iw + nx * ny] = T(0);
-                if (vb) a.out[Z][iw + nx * ny + 1] = T(0);
+                st_out(a.out[Z] + (iw + nx * ny), T(0));
+                if (vb) st_out(a.out[Z] + (iw + nx * ny + 1), T(0));
             }
         }
     }

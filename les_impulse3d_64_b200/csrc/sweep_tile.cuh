@@ -46,6 +46,15 @@ template <int TY, int TZ, int NT> struct TileGeom {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
+// A store of the sweep's results (the new impulse, stage 0's RK base) to global memory, issued as st.global: a
+// plain store through the arrays' generic pointers would, as far as the compiler can tell, alias the tile staged
+// in shared memory, and every staged value read after it would be loaded again.
+template <class T> __device__ __forceinline__ void st_out(T* p, T v) {
+    const size_t g = __cvta_generic_to_global(p);
+    if constexpr (sizeof(T) == 8) asm volatile("st.global.f64 [%0], %1;" ::"l"(g), "d"(v));
+    else asm volatile("st.global.f32 [%0], %1;" ::"l"(g), "f"(v));
+}
+
 template <int BYTES>
 __device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* src) {
     const unsigned int dst = (unsigned int)__cvta_generic_to_shared(smem_dst);
@@ -261,9 +270,18 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     auto w1 = [&](T okA, T okB, T lA, T lB) { return o4 ? okA * okB * (T(1) + (lA * lB) * eighth) : okA * okB; };
     auto w3 = [&](T lA, T lB) { return -((lA * lB) * eighth); };
 
+    // A warp takes RPT consecutive rows of one column of the tile: cells (y, z), (y, z + 1), ...  The three edges
+    // at a cell's lower corner each feed two of its faces with the narrow stencil (the z-edge at x-face x, y-face
+    // y its u- and v-faces; the y-edge at x-face x, z-face z its u- and w-faces; the x-edge at y-face y, z-face z
+    // its v- and w-faces), so each is evaluated once per cell; the y- and x-edges on z-face z + 1, which the
+    // cell's u- and v-faces reach, are the next row's corner edges and carry over in registers.  Every term is
+    // the same expression on the same operands as when each face evaluated its own.
+    static_assert(G::WARPS % TY == 0 && G::WARPS / TY * RPT == TZ, "a warp's rows are one column of the tile");
+    T cyWo = T(0), cyU = T(0), cyUl = T(0), cyUh = T(0);     // y-edge (x, z + 1): weighted omega_y, u-face term, u
+    T cxWo = T(0), cxV = T(0), cxVl = T(0), cxVh = T(0);     // x-edge (y, z + 1): weighted omega_x, v-face term, v
 #pragma unroll 1
     for (int k = 0; k < RPT; k++) {
-        const int row = warp + G::WARPS * k, ry = row % TY, rz = row / TY;
+        const int ry = warp % TY, rz = RPT * (warp / TY) + k;
         const int x = x0 + lane, y = y0 + ry, z = z0 + rz;
         if (x >= nx || y >= ny || z >= nz) continue;
         const T* pu = SU + ((rz + 3) * UH + ry + 3) * UW + lane + 1;   // u at x-face x, cells (y, z)
@@ -277,11 +295,60 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
         const T bu = rk ? __ldg(a.m0[X] + iu) : T(0), bv = rk ? __ldg(a.m0[Y] + iv) : T(0),
                 bw = rk ? __ldg(a.m0[Z] + iw) : T(0);
 
+        // ---------------- the corner edges: narrow terms of two faces each
+        T uZ0, vZ0, uY0, wY0, vX0, wX0, uY1, vX1;
+        {
+            const T ok1x = tX(kOk1, x), l1x = tX(kL1, x), i1x = tX(kInvSp, x), e1lx = tX(kEv1Lo, x), e1hx = tX(kEv1Hi, x);
+            const T ok1y = tY(kOk1, y), l1y = tY(kL1, y), i1y = tY(kInvSp, y), e1ly = tY(kEv1Lo, y), e1hy = tY(kEv1Hi, y);
+            const T e1lz = tZ(kEv1Lo, z), e1hz = tZ(kEv1Hi, z);
+            {   // z-edge (x, y): + w omega_z ev_x(v) on the u-face, - w omega_z ev_y(u) on the v-face
+                const T vl = pv[-1], vh = pv[0], ul = pu[-UW], uh = pu[0];
+                const T wo = w1(ok1x, ok1y, l1x, l1y) * ((vh - vl) * i1x - (uh - ul) * i1y);
+                uZ0 = wo * (e1lx * vl + e1hx * vh);
+                vZ0 = -(wo * (e1ly * ul + e1hy * uh));
+            }
+            if (k == 0) {
+                const T ok1z = tZ(kOk1, z), l1z = tZ(kL1, z), i1z = tZ(kInvSp, z);
+                {   // y-edge (x, z): - w omega_y ev_x(w) on the u-face, + w omega_y ev_z(u) on the w-face
+                    const T ul = pu[-UP], uh = pu[0], wl = pw[-1], wh = pw[0];
+                    const T wo = w1(ok1z, ok1x, l1z, l1x) * ((uh - ul) * i1z - (wh - wl) * i1x);
+                    uY0 = -(wo * (e1lx * wl + e1hx * wh));
+                    wY0 = wo * (e1lz * ul + e1hz * uh);
+                }
+                {   // x-edge (y, z): + w omega_x ev_y(w) on the v-face, - w omega_x ev_z(v) on the w-face
+                    const T wl = pw[-WW], wh = pw[0], vl = pv[-VP], vh = pv[0];
+                    const T wo = w1(ok1y, ok1z, l1y, l1z) * ((wh - wl) * i1y - (vh - vl) * i1z);
+                    vX0 = wo * (e1ly * wl + e1hy * wh);
+                    wX0 = -(wo * (e1lz * vl + e1hz * vh));
+                }
+            } else {     // the previous row's edges on this cell's lower z-face
+                uY0 = cyU;
+                wY0 = cyWo * (e1lz * cyUl + e1hz * cyUh);
+                vX0 = cxV;
+                wX0 = -(cxWo * (e1lz * cxVl + e1hz * cxVh));
+            }
+            {   // the edges on z-face z + 1 (the next row's corner edges)
+                const T ok1 = tZ(kOk1, z + 1), l1 = tZ(kL1, z + 1), i1 = tZ(kInvSp, z + 1);
+                const T ul = pu[0], uh = pu[UP], wl = pw[WP - 1], wh = pw[WP];
+                cyWo = w1(ok1, ok1x, l1, l1x) * ((uh - ul) * i1 - (wh - wl) * i1x);
+                cyU = -(cyWo * (e1lx * wl + e1hx * wh));
+                cyUl = ul;
+                cyUh = uh;
+                const T wl2 = pw[WP - WW], wh2 = pw[WP], vl = pv[0], vh = pv[VP];
+                cxWo = w1(ok1y, ok1, l1y, l1) * ((wh2 - wl2) * i1y - (vh - vl) * i1);
+                cxV = cxWo * (e1ly * wl2 + e1hy * wh2);
+                cxVl = vl;
+                cxVh = vh;
+            }
+            uY1 = cyU;
+            vX1 = cxV;
+        }
+
         // ---------------- u-face x: z-edges (b = Y, omega_z) and y-edges (b = Z, omega_y)
         {
             const int i = iu;
-            if (blend) a.m0_out[X][i] = MX[mo];
-            if (x == 0) a.out[X][i] = T(0);
+            if (blend) st_out(a.m0_out[X] + (i), MX[mo]);
+            if (x == 0) st_out(a.out[X] + (i), T(0));
             else {
                 const T ok1x = tX(kOk1, x), l1x = tX(kL1, x), l3x = tX(kL3, x), i1x = tX(kInvSp, x), i3x = tX(kInvNd3, x);
                 const T e1l = tX(kEv1Lo, x), e1h = tX(kEv1Hi, x), e3l = tX(kEv3Lo, x), e3h = tX(kEv3Hi, x);
@@ -298,38 +365,32 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                     const T wo = w3(l3x, tY(kL3, e)) * ((vh - vl) * i3x - (uh - ul) * tY(kInvNd3, e));
                     return wo * (e3l * vl + e3h * vh);
                 };
-                // y-edge at z-face e (d = e - z): - w omega_y ev_x(w)
-                auto py1 = [&](int d) {
-                    const int e = z + d;
-                    const T ul = pu[(d - 1) * UP], uh = pu[d * UP], wl = pw[d * WP - 1], wh = pw[d * WP];
-                    const T wo = w1(tZ(kOk1, e), ok1x, tZ(kL1, e), l1x) * ((uh - ul) * tZ(kInvSp, e) - (wh - wl) * i1x);
-                    return -(wo * (e1l * wl + e1h * wh));
-                };
+                // y-edge at z-face e (d = e - z): - w omega_y ev_x(w); the narrow ones are the corner edges
                 auto py3 = [&](int d) {
                     const int e = z + d;
                     const T ul = pu[(d - 2) * UP], uh = pu[(d + 1) * UP], wl = pw[d * WP - 2], wh = pw[d * WP + 1];
                     const T wo = w3(tZ(kL3, e), l3x) * ((uh - ul) * tZ(kInvNd3, e) - (wh - wl) * i3x);
                     return -(wo * (e3l * wl + e3h * wh));
                 };
-                T L = half * (pz1(1) + pz1(0)) + half * (py1(1) + py1(0));
+                T L = half * (pz1(1) + uZ0) + half * (uY1 + uY0);
                 if (o4) {
                     const T c3 = tX(kC3, x);
                     L = L + c3 * (pz3(2) + pz3(-1));
                     L = L + c3 * (py3(2) + py3(-1));
                 }
                 L = L - (kc - Kc[kidx(lane, ry + 1, rz + 1)]) * tX(kInvSp, x);
-                a.out[X][i] = viscous_rk_tile<X, T, MW, MH>(a, MX + mo, pu[0], sc, dt, lidv, x, y, z, bu, L, tX, tY, tZ);
+                st_out(a.out[X] + (i), viscous_rk_tile<X, T, MW, MH>(a, MX + mo, pu[0], sc, dt, lidv, x, y, z, bu, L, tX, tY, tZ));
             }
             if (x == nx - 1) {
-                if (blend) a.m0_out[X][i + 1] = MX[mo + 1];
-                a.out[X][i + 1] = T(0);
+                if (blend) st_out(a.m0_out[X] + (i + 1), MX[mo + 1]);
+                st_out(a.out[X] + (i + 1), T(0));
             }
         }
         // ---------------- v-face y: z-edges (b = X, omega_z) and x-edges (b = Z, omega_x)
         {
             const int i = iv;
-            if (blend) a.m0_out[Y][i] = MY[mo];
-            if (y == 0) a.out[Y][i] = T(0);
+            if (blend) st_out(a.m0_out[Y] + (i), MY[mo]);
+            if (y == 0) st_out(a.out[Y] + (i), T(0));
             else {
                 const T ok1y = tY(kOk1, y), l1y = tY(kL1, y), l3y = tY(kL3, y), i1y = tY(kInvSp, y), i3y = tY(kInvNd3, y);
                 const T e1l = tY(kEv1Lo, y), e1h = tY(kEv1Hi, y), e3l = tY(kEv3Lo, y), e3h = tY(kEv3Hi, y);
@@ -346,38 +407,32 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                     const T wo = w3(tX(kL3, e), l3y) * ((vh - vl) * tX(kInvNd3, e) - (uh - ul) * i3y);
                     return -(wo * (e3l * ul + e3h * uh));
                 };
-                // x-edge at z-face e (d = e - z): + w omega_x ev_y(w)
-                auto px1 = [&](int d) {
-                    const int e = z + d;
-                    const T wl = pw[d * WP - WW], wh = pw[d * WP], vl = pv[(d - 1) * VP], vh = pv[d * VP];
-                    const T wo = w1(ok1y, tZ(kOk1, e), l1y, tZ(kL1, e)) * ((wh - wl) * i1y - (vh - vl) * tZ(kInvSp, e));
-                    return wo * (e1l * wl + e1h * wh);
-                };
+                // x-edge at z-face e (d = e - z): + w omega_x ev_y(w); the narrow ones are the corner edges
                 auto px3 = [&](int d) {
                     const int e = z + d;
                     const T wl = pw[d * WP - 2 * WW], wh = pw[d * WP + WW], vl = pv[(d - 2) * VP], vh = pv[(d + 1) * VP];
                     const T wo = w3(l3y, tZ(kL3, e)) * ((wh - wl) * i3y - (vh - vl) * tZ(kInvNd3, e));
                     return wo * (e3l * wl + e3h * wh);
                 };
-                T L = half * (pz1(1) + pz1(0)) + half * (px1(1) + px1(0));
+                T L = half * (pz1(1) + vZ0) + half * (vX1 + vX0);
                 if (o4) {
                     const T c3 = tY(kC3, y);
                     L = L + c3 * (pz3(2) + pz3(-1));
                     L = L + c3 * (px3(2) + px3(-1));
                 }
                 L = L - (kc - Kc[kidx(lane + 1, ry, rz + 1)]) * tY(kInvSp, y);
-                a.out[Y][i] = viscous_rk_tile<Y, T, MW, MH>(a, MY + mo, pv[0], sc, dt, lidv, x, y, z, bv, L, tX, tY, tZ);
+                st_out(a.out[Y] + (i), viscous_rk_tile<Y, T, MW, MH>(a, MY + mo, pv[0], sc, dt, lidv, x, y, z, bv, L, tX, tY, tZ));
             }
             if (y == ny - 1) {
-                if (blend) a.m0_out[Y][i + nx] = MY[mo + MW];
-                a.out[Y][i + nx] = T(0);
+                if (blend) st_out(a.m0_out[Y] + (i + nx), MY[mo + MW]);
+                st_out(a.out[Y] + (i + nx), T(0));
             }
         }
         // ---------------- w-face z: x-edges (b = Y, omega_x) and y-edges (b = X, omega_y)
         {
             const int i = iw;
-            if (blend) a.m0_out[Z][i] = MZ[mo];
-            if (z == 0) a.out[Z][i] = T(0);
+            if (blend) st_out(a.m0_out[Z] + (i), MZ[mo]);
+            if (z == 0) st_out(a.out[Z] + (i), T(0));
             else {
                 const T ok1z = tZ(kOk1, z), l1z = tZ(kL1, z), l3z = tZ(kL3, z), i1z = tZ(kInvSp, z), i3z = tZ(kInvNd3, z);
                 const T e1l = tZ(kEv1Lo, z), e1h = tZ(kEv1Hi, z), e3l = tZ(kEv3Lo, z), e3h = tZ(kEv3Hi, z);
@@ -407,30 +462,30 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
                     const T wo = w3(l3z, tX(kL3, e)) * ((uh - ul) * i3z - (wh - wl) * tX(kInvNd3, e));
                     return wo * (e3l * ul + e3h * uh);
                 };
-                T L = half * (px1(1) + px1(0)) + half * (py1(1) + py1(0));
+                T L = half * (px1(1) + wX0) + half * (py1(1) + wY0);
                 if (o4) {
                     const T c3 = tZ(kC3, z);
                     L = L + c3 * (px3(2) + px3(-1));
                     L = L + c3 * (py3(2) + py3(-1));
                 }
                 L = L - (kc - Kc[kidx(lane + 1, ry + 1, rz)]) * tZ(kInvSp, z);
-                a.out[Z][i] = viscous_rk_tile<Z, T, MW, MH>(a, MZ + mo, pw[0], sc, dt, lidv, x, y, z, bw, L, tX, tY, tZ);
+                st_out(a.out[Z] + (i), viscous_rk_tile<Z, T, MW, MH>(a, MZ + mo, pw[0], sc, dt, lidv, x, y, z, bw, L, tX, tY, tZ));
             }
             if (z == nz - 1) {
-                if (blend) a.m0_out[Z][i + nx * ny] = MZ[mo + MW * MH];
-                a.out[Z][i + nx * ny] = T(0);
+                if (blend) st_out(a.m0_out[Z] + (i + nx * ny), MZ[mo + MW * MH]);
+                st_out(a.out[Z] + (i + nx * ny), T(0));
             }
         }
     }
 }
 
 template <class T, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) sweep_tile_kernel(MomentumArgs<T> a) {
+__global__ void __launch_bounds__(NT, 2) sweep_tile_kernel(MomentumArgs<T> a) {
     sweep_tile_body<T, TY, TZ, NT>(a, real_blk());
 }
 // a batch of cavities: grid x runs over the work list (BatchItem)
 template <class T, int TY, int TZ, int NT>
-__global__ void __launch_bounds__(NT) sweep_tile_batched(const MomentumArgs<T>* args, const BatchItem* items,
+__global__ void __launch_bounds__(NT, 2) sweep_tile_batched(const MomentumArgs<T>* args, const BatchItem* items,
                                                           const int* live) {
     __shared__ MomentumArgs<T> a;
     int cav;
