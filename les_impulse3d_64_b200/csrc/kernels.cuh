@@ -282,17 +282,32 @@ __device__ bool publish_partials(const Vec<N>& blk, double* partial, unsigned in
     return publish_partials(blk, partial, counter, real_blk());
 }
 
-// In the last block: reduce all partials in a fixed order.  Result valid in thread 0.
+// In the last block: reduce all partials in a fixed order (thread t combines the partials of blocks t, t + NT,
+// t + 2 NT, ... in that order, then the block reduces).  Result valid in thread 0.  The loads of all N sums and
+// of four block indices per thread are issued together before any is combined: this reduction is the tail of
+// every reducing kernel, and the next kernel waits for it, so it should cost one L2 round trip per four
+// indices, not one per sum and index.
 template <int N, bool MAX>
 __device__ Vec<N> final_reduce(const double* partial, const Blk& k) {
-    const unsigned int nblocks = k.nx * k.ny;
+    constexpr int U = 4;
+    const unsigned int nblocks = k.nx * k.ny, nt = blockDim.x;
     Vec<N> acc;
 #pragma unroll
-    for (int k = 0; k < N; k++) {
-        double a = MAX ? -INFINITY : 0.0;
-        for (unsigned int i = threadIdx.x; i < nblocks; i += blockDim.x)
-            a = combine<N, MAX>(a, __ldcg(partial + k * nblocks + i));
-        acc.v[k] = a;
+    for (int j = 0; j < N; j++) acc.v[j] = MAX ? -INFINITY : 0.0;
+    for (unsigned int base = threadIdx.x; base < nblocks; base += U * nt) {
+        double v[U][N];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const unsigned int i = base + u * nt;
+#pragma unroll
+            for (int j = 0; j < N; j++) v[u][j] = i < nblocks ? __ldcg(partial + j * nblocks + i) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (base + u * nt >= nblocks) break;
+#pragma unroll
+            for (int j = 0; j < N; j++) acc.v[j] = combine<N, MAX>(acc.v[j], v[u][j]);
+        }
     }
     return block_reduce<N, MAX>(acc);
 }

@@ -10,10 +10,11 @@
 //   - the slices of the per-axis coefficient tables the tile uses.
 // No thread waits on a global load while staging: every element is a cp.async, all in flight together.
 // Staged values outside the box are clamped copies; every stencil term that reaches them has weight zero.
-// K = u.m (backend.cu:218-222) is computed once per cell.  Each face then evaluates its eight edge terms
-// (vorticity times interpolated velocity: backend.cu:141-215) from shared memory and adds them in the
+// K = u.m (backend.cu:218-222) is computed once per cell.  Each face then adds its eight edge terms
+// (vorticity times interpolated velocity: backend.cu:141-215), evaluated from shared memory, in the
 // reference's order: narrow then wide stencil, first then second tangential axis (backend.cu:232-238,
-// 249-255, 266-272).  It then adds -grad K, the viscous flux Laplacian with its wall and lid fluxes, and the RK
+// 249-255, 266-272).  The narrow terms of the three edges at a cell's lower corner, each shared by two of its
+// faces, are evaluated once per cell, and those on its upper z-face carry over to the cell above.  It then adds -grad K, the viscous flux Laplacian with its wall and lid fluxes, and the RK
 // combination (backend.cu:279-330).  The validity rules of the reference's stencils are folded into the weight
 // tables (kOk1, kL1, kL3), so the edge arithmetic has no branches.
 #pragma once
