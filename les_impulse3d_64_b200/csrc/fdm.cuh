@@ -171,6 +171,7 @@ constexpr int kPairThreads = 256;
 
 struct FdmPairArgs {
     int nx, ny, nz, clear_condition;
+    int per;                        // tiles per CTA (pair_per); the CTA's first tile is its block index times per
     const double* s[3];
     const double* st[3];
     const double* inv_lambda;
@@ -256,7 +257,12 @@ template <int W> struct PairSmem {
     static constexpr size_t bytes = sizeof(double) * (2 * kPairMax * kPairPitch + 2 * kPairMax * kPanel);
 };
 
-// t[z] = ST_y (r[z] S_x) on columns [x0, x0 + W) of plane z: transforms 1 and 2 of the pass
+// A CTA of a paired launch takes `a.per` consecutive tiles that share their bases (the z-planes of one column or
+// row block, or consecutive plane-column blocks): the bases are staged once, and each next tile's field is copied
+// under the current tile's second transform, into the buffer its first transform has finished reading.  A single
+// cavity's launch has one tile per CTA; a large batch's launch several (pair_per).
+
+// t[z] = ST_y (r[z] S_x) on columns [x0, x0 + W) of planes z: transforms 1 and 2 of the pass
 template <int W>
 __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     pair_begin(a, first, true);
@@ -266,7 +272,8 @@ __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     double* A2 = A1 + kPairMax * kPairPitch;        // ST_y: ny x ny
     double* B1 = A2 + kPairMax * kPairPitch;        // S_x[:, x0 .. x0 + W)
     double* C1 = B1 + kPairMax * PW;                // r[z] S_x on those columns
-    const int nx = a.nx, ny = a.ny, z = blk.y, x0 = blk.x * W;
+    const int nx = a.nx, ny = a.ny, x0 = blk.x * W;
+    const int z0 = blk.y * a.per, z1 = min(a.nz, z0 + a.per);
     const int my = round_up(ny, 8), kx = round_up(nx, 4), ky = round_up(ny, 4);
     pair_stage<W / 2>(B1, PW, a.s[X] + x0, nx, nx, min(W, nx - x0), kx, W);
     pair_stage<32>(A2, kPairPitch, a.st[Y], ny, ny, ny, my, ky);
@@ -275,38 +282,48 @@ __device__ void pair_xy_body(const FdmPairArgs& a, const Blk& blk, bool first) {
         cp_async_wait<0>();
         return;
     }
-    const double* r = (a.r_alt && a.c->use_rhs ? a.r_alt : a.r) + (long long)z * nx * ny;
-    pair_stage<32>(A1, kPairPitch, r, nx, ny, nx, my, kx);
+    const double* r = a.r_alt && a.c->use_rhs ? a.r_alt : a.r;
+    pair_stage<32>(A1, kPairPitch, r + (long long)z0 * nx * ny, nx, ny, nx, my, kx);
     cp_async_commit();
     cp_async_wait<0>();
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = warp * 8;                        // the warp's 8 rows (y) x W columns
-    double acc[1][FN][2];
-    if (m0 < my) {
-        pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, PW, kx, m0, 0);
+    for (int z = z0; z < z1; z++) {
+        double acc[1][FN][2];
+        if (m0 < my) {
+            pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, PW, kx, m0, 0);
 #pragma unroll
-        for (int j = 0; j < FN; j++) {
-            C1[(m0 + fr) * PW + j * 8 + 2 * fc] = acc[0][j][0];
-            C1[(m0 + fr) * PW + j * 8 + 2 * fc + 1] = acc[0][j][1];
+            for (int j = 0; j < FN; j++) {
+                C1[(m0 + fr) * PW + j * 8 + 2 * fc] = acc[0][j][0];
+                C1[(m0 + fr) * PW + j * 8 + 2 * fc + 1] = acc[0][j][1];
+            }
         }
+        __syncthreads();
+        if (z + 1 < z1) {
+            pair_stage<32>(A1, kPairPitch, r + (long long)(z + 1) * nx * ny, nx, ny, nx, my, kx);
+            cp_async_commit();
+        }
+        const int y = m0 + fr;
+        if (m0 < my) {
+            pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, ky, m0, 0);
+            if (y < ny) {
+                double* t = a.t + ((long long)z * ny + y) * nx;
+#pragma unroll
+                for (int j = 0; j < FN; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int x = x0 + j * 8 + 2 * fc + h;
+                        if (x < nx) t[x] = acc[0][j][h];
+                    }
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();
     }
-    __syncthreads();
-    if (m0 >= my) return;
-    pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, ky, m0, 0);
-    const int y = m0 + fr;
-    if (y >= ny) return;
-    double* t = a.t + ((long long)z * ny + y) * nx;
-#pragma unroll
-    for (int j = 0; j < FN; j++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int x = x0 + j * 8 + 2 * fc + h;
-            if (x < nx) t[x] = acc[0][j][h];
-        }
 }
 
-// t[:, c] = S_z (inv_lambda .* (ST_z t[:, c])) on plane columns c in [c0, c0 + W), in place: transforms 3 and 4
+// t[:, c] = S_z (inv_lambda .* (ST_z t[:, c])) on plane columns c of blocks of W, in place: transforms 3 and 4
 template <int W>
 __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     pair_begin(a, first, false);
@@ -316,10 +333,11 @@ __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     double* A2 = A1 + kPairMax * kPairPitch;        // S_z
     double* B1 = A2 + kPairMax * kPairPitch;        // t[:, c0 .. c0 + W)
     double* C1 = B1 + kPairMax * PW;
-    const int nz = a.nz, plane = a.nx * a.ny, c0 = blk.x * W;
+    const int nz = a.nz, plane = a.nx * a.ny;
+    const int nb = (plane + W - 1) / W, b0 = blk.x * a.per, b1 = min(nb, b0 + a.per);
     const int mz = round_up(nz, 8), kz = round_up(nz, 4);
     pair_stage<32>(A1, kPairPitch, a.st[Z], nz, nz, nz, mz, kz);
-    pair_stage<W / 2>(B1, PW, a.t + c0, plane, nz, min(W, plane - c0), kz, W);
+    pair_stage<W / 2>(B1, PW, a.t + b0 * W, plane, nz, min(W, plane - b0 * W), kz, W);
     cp_async_commit();
     pair_stage<32>(A2, kPairPitch, a.s[Z], nz, nz, nz, mz, kz);
     cp_async_commit();
@@ -329,43 +347,54 @@ __device__ void pair_z_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, fr = lane >> 2, fc = lane & 3;
     const int m0 = warp * 8;
-    double acc[1][FN][2], il[FN][2];
-    if (m0 < mz) {
-        const int z = m0 + fr;
+    for (int b = b0; b < b1; b++) {
+        const int c0 = b * W;
+        double acc[1][FN][2], il[FN][2];
+        if (m0 < mz) {
+            const int z = m0 + fr;
 #pragma unroll
-        for (int j = 0; j < FN; j++)
+            for (int j = 0; j < FN; j++)
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int c = c0 + j * 8 + 2 * fc + h;
-                il[j][h] = z < nz && c < plane ? __ldg(a.inv_lambda + (long long)z * plane + c) : 0.0;
-            }
-    }
-    cp_async_wait<1>();
-    __syncthreads();
-    if (m0 < mz) {
-        pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, PW, kz, m0, 0);
-#pragma unroll
-        for (int j = 0; j < FN; j++)
-#pragma unroll
-            for (int h = 0; h < 2; h++) C1[(m0 + fr) * PW + j * 8 + 2 * fc + h] = acc[0][j][h] * il[j][h];
-    }
-    cp_async_wait<0>();
-    __syncthreads();
-    if (m0 >= mz) return;
-    pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, kz, m0, 0);
-    const int z = m0 + fr;
-    if (z >= nz) return;
-    double* t = a.t + (long long)z * plane;
-#pragma unroll
-    for (int j = 0; j < FN; j++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int c = c0 + j * 8 + 2 * fc + h;
-            if (c < plane) t[c] = acc[0][j][h];
+                for (int h = 0; h < 2; h++) {
+                    const int c = c0 + j * 8 + 2 * fc + h;
+                    il[j][h] = z < nz && c < plane ? __ldg(a.inv_lambda + (long long)z * plane + c) : 0.0;
+                }
         }
+        if (b == b0) cp_async_wait<1>();             // ST_z and the first block (S_z may still be in flight)
+        __syncthreads();
+        if (m0 < mz) {
+            pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, PW, kz, m0, 0);
+#pragma unroll
+            for (int j = 0; j < FN; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) C1[(m0 + fr) * PW + j * 8 + 2 * fc + h] = acc[0][j][h] * il[j][h];
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+        if (b + 1 < b1) {
+            pair_stage<W / 2>(B1, PW, a.t + c0 + W, plane, nz, min(W, plane - c0 - W), kz, W);
+            cp_async_commit();
+        }
+        const int z = m0 + fr;
+        if (m0 < mz) {
+            pair_warp_mma<1, FN>(acc, A2, kPairPitch, C1, PW, kz, m0, 0);
+            if (z < nz) {
+                double* t = a.t + (long long)z * plane;
+#pragma unroll
+                for (int j = 0; j < FN; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int c = c0 + j * 8 + 2 * fc + h;
+                        if (c < plane) t[c] = acc[0][j][h];
+                    }
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();
+    }
 }
 
-// phi[z] += (S_y t[z]) ST_x on rows [y0, y0 + W) of plane z: transforms 5 and 6
+// phi[z] += (S_y t[z]) ST_x on rows [y0, y0 + W) of planes z: transforms 5 and 6
 template <int W>
 __device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     pair_begin(a, first, false);
@@ -375,11 +404,12 @@ __device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     double* B2 = B1 + kPairMax * kPairPitch;        // ST_x: nx x nx
     double* A1 = B2 + kPairMax * kPairPitch;        // S_y[y0 .. y0 + W, :]
     double* C1 = A1 + W * kPairPitch;               // S_y t[z] on those rows
-    const int nx = a.nx, ny = a.ny, z = blk.y, y0 = blk.x * W;
+    const int nx = a.nx, ny = a.ny, y0 = blk.x * W;
+    const int z0 = blk.y * a.per, z1 = min(a.nz, z0 + a.per);
     const int kx = round_up(nx, 4), ky = round_up(ny, 4), mx = round_up(nx, 8);
     const int cx = min(kPairMax, round_up(mx, 8 * FN));      // columns the active warps read: staged, zero past nx
     pair_stage<32>(A1, kPairPitch, a.s[Y] + (long long)y0 * ny, ny, min(W, ny - y0), ny, W, ky);
-    pair_stage<32>(B1, kPairPitch, a.t + (long long)z * nx * ny, nx, ny, nx, ky, cx);
+    pair_stage<32>(B1, kPairPitch, a.t + (long long)z0 * nx * ny, nx, ny, nx, ky, cx);
     cp_async_commit();
     pair_stage<32>(B2, kPairPitch, a.st[X], nx, nx, nx, kx, cx);
     cp_async_commit();
@@ -392,38 +422,48 @@ __device__ void pair_yx_body(const FdmPairArgs& a, const Blk& blk, bool first) {
     const bool active = n0 < mx;
     const int y = y0 + m0 + fr;
     const int reset = a.c->reset_phi;
-    double* phi = a.phi + ((long long)z * ny + min(y, ny - 1)) * nx;
-    double old[FN][2];                              // the potential this thread updates, loaded ahead
+    for (int z = z0; z < z1; z++) {
+        double* phi = a.phi + ((long long)z * ny + min(y, ny - 1)) * nx;
+        double old[FN][2];                          // the potential this thread updates, loaded ahead
 #pragma unroll
-    for (int j = 0; j < FN; j++)
+        for (int j = 0; j < FN; j++)
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int x = n0 + j * 8 + 2 * fc + h;
-            old[j][h] = active && y < ny && x < nx && !reset ? phi[x] : 0.0;
+            for (int h = 0; h < 2; h++) {
+                const int x = n0 + j * 8 + 2 * fc + h;
+                old[j][h] = active && y < ny && x < nx && !reset ? phi[x] : 0.0;
+            }
+        if (z == z0) cp_async_wait<1>();             // S_y and the first plane (ST_x may still be in flight)
+        __syncthreads();
+        double acc[1][FN][2];
+        if (active) {
+            pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, kPairPitch, ky, m0, n0);
+#pragma unroll
+            for (int j = 0; j < FN; j++) {
+                C1[(m0 + fr) * kPairPitch + n0 + j * 8 + 2 * fc] = acc[0][j][0];
+                C1[(m0 + fr) * kPairPitch + n0 + j * 8 + 2 * fc + 1] = acc[0][j][1];
+            }
         }
-    cp_async_wait<1>();
-    __syncthreads();
-    double acc[1][FN][2];
-    if (active) {
-        pair_warp_mma<1, FN>(acc, A1, kPairPitch, B1, kPairPitch, ky, m0, n0);
-#pragma unroll
-        for (int j = 0; j < FN; j++) {
-            C1[(m0 + fr) * kPairPitch + n0 + j * 8 + 2 * fc] = acc[0][j][0];
-            C1[(m0 + fr) * kPairPitch + n0 + j * 8 + 2 * fc + 1] = acc[0][j][1];
+        cp_async_wait<0>();
+        __syncthreads();
+        if (z + 1 < z1) {
+            pair_stage<32>(B1, kPairPitch, a.t + (long long)(z + 1) * nx * ny, nx, ny, nx, ky, cx);
+            cp_async_commit();
         }
+        if (active) {
+            pair_warp_mma<1, FN>(acc, C1, kPairPitch, B2, kPairPitch, kx, m0, n0);
+            if (y < ny) {
+#pragma unroll
+                for (int j = 0; j < FN; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int x = n0 + j * 8 + 2 * fc + h;
+                        if (x < nx) phi[x] = old[j][h] + acc[0][j][h];
+                    }
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();
     }
-    cp_async_wait<0>();
-    __syncthreads();
-    if (!active) return;
-    pair_warp_mma<1, FN>(acc, C1, kPairPitch, B2, kPairPitch, kx, m0, n0);
-    if (y >= ny) return;
-#pragma unroll
-    for (int j = 0; j < FN; j++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int x = n0 + j * 8 + 2 * fc + h;
-            if (x < nx) phi[x] = old[j][h] + acc[0][j][h];
-        }
 }
 template <int W> struct PairYxSmem {
     static constexpr size_t bytes = sizeof(double) * (2 * kPairMax * kPairPitch + 2 * W * kPairPitch);
@@ -460,11 +500,11 @@ inline size_t pair_smem_bytes(int phase, int w) {
     if (w == 16) return phase == kPairYx ? PairYxSmem<16>::bytes : PairSmem<16>::bytes;
     return phase == kPairYx ? PairYxSmem<32>::bytes : PairSmem<32>::bytes;
 }
-// grid of one phase for an nx x ny x nz cavity with CTA width w
-inline dim3 pair_grid(int phase, int w, int nx, int ny, int nz) {
-    if (phase == kPairXy) return dim3((nx + w - 1) / w, nz);
-    if (phase == kPairZ) return dim3((nx * ny + w - 1) / w);
-    return dim3((ny + w - 1) / w, nz);
+// grid of one phase for an nx x ny x nz cavity with CTA width w and `per` tiles per CTA
+inline dim3 pair_grid(int phase, int w, int nx, int ny, int nz, int per = 1) {
+    if (phase == kPairXy) return dim3((nx + w - 1) / w, (nz + per - 1) / per);
+    if (phase == kPairZ) return dim3(((nx * ny + w - 1) / w + per - 1) / per);
+    return dim3((ny + w - 1) / w, (nz + per - 1) / per);
 }
 inline bool pair_pass_fits(int nx, int ny, int nz) {
     return nx <= kPairMax && ny <= kPairMax && nz <= kPairMax;
@@ -487,6 +527,30 @@ inline int pair_width(int nx, int nz) {
     if (g_launch_record) return 32;
     const long long ctas = (long long)((nx + 31) / 32) * nz;
     return ctas < sms ? 16 : 32;
+}
+// Tiles per CTA of a paired launch: one for a single cavity; in a batch as many as leave the whole launch (all its
+// cavities counted at this one's size) three to four waves of two CTAs per SM, evened out over the axis, so that a
+// CTA stages its bases once for several tiles and copies each next tile's field under the current tile's
+// arithmetic.  For 64 cavities of 64^3 that is 8 planes per CTA: the batch's first passes took 2.15 ms per step
+// against 2.51 with one tile per CTA, 2.19 with 4 and 2.35 with 16.  At most 8 tiles per CTA, so that in a batch of
+// mixed sizes (each member counted at its own size) no CTA holds much more work than that.  CAVITY_PAIR_PER forces
+// it.
+inline int pair_per(int phase, int w, int nx, int ny, int nz) {
+    static const int forced = [] {
+        const char* e = std::getenv("CAVITY_PAIR_PER");
+        return e ? std::atoi(e) : 0;
+    }();
+    static const int sms = current_sm_count();
+    const dim3 g = pair_grid(phase, w, nx, ny, nz, 1);
+    const int along = phase == kPairZ ? (int)g.x : nz;      // the tiles one CTA can take in a row
+    int per = forced;
+    if (per <= 0) {
+        const long long tiles = (long long)g.x * g.y * std::max(g_launch_batch, 1);
+        per = (int)std::min<long long>(std::min(along, 8), std::max(1LL, tiles / (6LL * sms)));
+        const int chunks = (along + per - 1) / per;
+        per = (along + chunks - 1) / chunks;
+    }
+    return std::max(1, std::min(per, along));
 }
 template <int W> inline cudaError_t pair_prepare_w() {
     cudaError_t r = cudaFuncSetAttribute(pair_xy_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -531,7 +595,8 @@ inline void launch_fdm_pass_pairs(cudaStream_t st, const FdmOperands& op, const 
     a.r = r; a.r_alt = r_alt; a.t = t; a.phi = phi; a.c = c; a.handle = h;
     const int w = pair_width(op.nx, op.nz);
     for (int ph = 0; ph < 3; ph++) {
-        const dim3 grid = pair_grid(ph, w, op.nx, op.ny, op.nz);
+        a.per = pair_per(ph, w, op.nx, op.ny, op.nz);
+        const dim3 grid = pair_grid(ph, w, op.nx, op.ny, op.nz, a.per);
         if (record_launch(kLkPair, ph | (w << 4), grid, pair_smem_bytes(ph, w), a)) continue;
         if (w == 16) launch_pair_w<16>(ph, grid, st, a);
         else launch_pair_w<32>(ph, grid, st, a);

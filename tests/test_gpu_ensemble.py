@@ -72,6 +72,43 @@ def test_large_mixed_size_batch_matches_alone(group):
             assert err <= 1e-6, (i, k, err)
 
 
+BATCH_RUN = r'''
+import sys
+import numpy as np
+sys.path[:0] = [{root!r}]
+from les_impulse3d_64_b200 import workloads
+from les_impulse3d_64_b200.ensemble import Ensemble
+cases = workloads.ensemble_cases(count=6, seed=13, sizes=(24, 40, 64), re_range=(100.0, 2000.0))
+for k, c in enumerate(cases):
+    c['precision'] = 'mixed' if k % 2 else 'fp64'
+ens = Ensemble(cases, group='precision')
+ens.advance(3, chunk=3)
+np.savez({path!r}, **{{f'{{i}}_{{k}}': v for i in range(len(cases)) for k, v in ens.fields(i).items()}})
+ens.close()
+print('ok')
+'''
+
+
+def test_batch_pass_tiles_per_cta(tmp_path):
+    """A batch of cavities of three sizes in both forms whose paired FP64 passes take one tile per CTA, or four
+    (CAVITY_PAIR_PER, read once per process: a child process each): the same fields bit for bit."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    out = {}
+    for per in ('1', '4'):
+        path = str(tmp_path / f'per{per}.npz')
+        env = dict(os.environ, CAVITY_PAIR_PER=per)
+        res = subprocess.run([sys.executable, '-c', BATCH_RUN.format(root=str(root), path=path)], env=env,
+                             capture_output=True, text=True, timeout=600)
+        assert res.returncode == 0 and 'ok' in res.stdout, res.stdout + res.stderr
+        out[per] = np.load(path)
+    for k in out['1'].files:
+        assert np.array_equal(out['1'][k], out['4'][k]), k
+
+
 @pytest.mark.parametrize('form', ['0', '2'])
 def test_batch_pass_forms_agree(form):
     """A batch of cavities of three sizes with its FP64 passes as six launches (CAVITY_FDM_FUSED=0, the large and

@@ -183,6 +183,22 @@ def test_paired_pass_widths(width):
     assert res.returncode == 0 and 'ok' in res.stdout, res.stdout + res.stderr
 
 
+@pytest.mark.parametrize('per', ['3', '64'])
+def test_paired_pass_tiles_per_cta(per):
+    """The paired pass with several tiles per CTA (CAVITY_PAIR_PER: planes, or plane-column blocks, taken in a row
+    by one CTA with its bases staged once, as large batches run it; read once per process: a child process each),
+    the last CTA of an axis taking fewer, equals the six-launch pass bit for bit."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    tests = Path(__file__).resolve().parent
+    code = WIDTH_CHECK.format(tests=str(tests), root=str(tests.parent))
+    env = dict(os.environ, CAVITY_PAIR_PER=per)
+    res = subprocess.run([sys.executable, '-c', code], env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0 and 'ok' in res.stdout, res.stdout + res.stderr
+
+
 TC_KERNEL_RUN = r'''
 import sys
 import numpy as np
