@@ -163,9 +163,17 @@ def profile_traffic(workload):
     return None
 
 
-def sweep_kernel_name():
-    """The momentum-sweep kernel the library runs: the shared-memory tile kernel unless CAVITY_SWEEP=face."""
-    return 'momentum_kernel' if os.environ.get('CAVITY_SWEEP') == 'face' else 'sweep_tile_kernel'
+def sweep_kernel_name(precision):
+    """The momentum-sweep kernel the library runs: the shared-memory tile kernel in the FP64 form and its packed
+    two-cells-per-thread variant in the mixed form, unless CAVITY_SWEEP selects another."""
+    kind = os.environ.get('CAVITY_SWEEP', '')
+    if kind == 'face':
+        return 'momentum_kernel'
+    if kind == 'march':
+        return 'sweep_march_kernel'
+    if kind == 'tile' or precision == 'fp64':
+        return 'sweep_tile_kernel'
+    return 'sweep_pair_kernel'
 
 
 def momentum_bytes(settings, field_bytes):
@@ -435,7 +443,7 @@ def run_ours(args, ranks):
                                'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
         'gpu_launches': launches,
         'pressure_passes_per_stage': passes / (3 * (2 * args.steps + args.warmup)) if args.steps else None,
-        'roofline': {'kernel': sweep_kernel_name(), 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+        'roofline': {'kernel': sweep_kernel_name(precision), 'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                      'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': profile_traffic(args.workload), 'ms_per_launch': kernel_s * 1e3},
         'stencil_kernels': cell_kernels,
