@@ -195,7 +195,7 @@ template <class T> class Solver : public SolverBase {
     using TileG = TileGeom<kTileTY, kTileTZ, kTileNT>;
     // the FP32 tile sweep with two cells per thread in packed arithmetic (sweep_pair.cuh): the same tile, 256 threads
     static constexpr int kPairNT = 256;
-    using PairG = TileGeom<kTileTY, kTileTZ, kPairNT>;
+    using PairG = TileGeom<kTileTY, kTileTZ, kPairNT, true>;
     // the z-march sweep (sweep_march.cuh): 32 x 8 columns of cells per CTA
     static constexpr int kMarchTX = 32, kMarchTY = 8;
     using MarchG = MarchGeom<kMarchTX, kMarchTY>;

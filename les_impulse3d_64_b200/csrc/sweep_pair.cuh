@@ -92,7 +92,7 @@ __device__ __forceinline__ F2 viscous_rk_pair(const MomentumArgs<float>& a, cons
 template <int TY, int TZ, int NT>
 __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
     using T = float;
-    using G = TileGeom<TY, TZ, NT>;
+    using G = TileGeom<TY, TZ, NT, true>;           // odd row pitches: a warp reads two rows (half warps)
     constexpr int TX = G::TX;
     constexpr int UW = G::UW, UH = G::UH, VW = G::VW, VH = G::VH, WW = G::WW, WH = G::WH, MW = G::MW, MH = G::MH;
     constexpr int UP = UH * UW, VP = VH * VW, WP = WH * WW;
@@ -102,7 +102,7 @@ __device__ void sweep_pair_body(const MomentumArgs<float>& a, const Blk& blk) {
     const TileArrays<T> ta = tile_arrays<T, G>(smem_raw);
     StageConst sc;
     T dt;
-    if (!tile_prologue<T, TY, TZ, NT>(a, blk, ta, sc, dt)) return;
+    if (!tile_prologue<T, G>(a, blk, ta, sc, dt)) return;
     const T *SU = ta.SU, *SV = ta.SV, *SW = ta.SW, *MX = ta.MX, *MY = ta.MY, *MZ = ta.MZ, *Kc = ta.Kc;
     const Params& p = a.p;
     const int nx = p.nx, ny = p.ny, nz = p.nz;

@@ -14,28 +14,36 @@
 // (vorticity times interpolated velocity: backend.cu:141-215), evaluated from shared memory, in the
 // reference's order: narrow then wide stencil, first then second tangential axis (backend.cu:232-238,
 // 249-255, 266-272).  The narrow terms of the three edges at a cell's lower corner, each shared by two of its
-// faces, are evaluated once per cell, and those on its upper z-face carry over to the cell above.  It then adds -grad K, the viscous flux Laplacian with its wall and lid fluxes, and the RK
-// combination (backend.cu:279-330).  The validity rules of the reference's stencils are folded into the weight
-// tables (kOk1, kL1, kL3), so the edge arithmetic has no branches.
+// faces, are evaluated once per cell, and those on its upper z-face carry over to the cell above.  It then adds
+// -grad K, the viscous flux Laplacian with its wall and lid fluxes, and the RK combination (backend.cu:279-330).
+// The validity rules of the reference's stencils are folded into the weight tables (kOk1, kL1, kL3), so the edge
+// arithmetic has no branches.
 #pragma once
 #include "sweep.cuh"
 
 namespace cavity {
 
-// TY x TZ rows of 32 cells per CTA, NT threads (one warp per row at a time)
-template <int TY, int TZ, int NT> struct TileGeom {
+// TY x TZ rows of 32 cells per CTA, NT threads (one warp per row at a time).  ODD: every staged box gets an odd
+// row pitch (one unused column where its width is even), for a kernel whose warps read two rows at once, each half
+// warp every other word of its row (sweep_pair.cuh): with an even pitch both halves land on the same 16 banks and
+// every such load takes two shared-memory wavefronts instead of one.
+template <int TY, int TZ, int NT, bool ODD = false> struct TileGeom {
     static constexpr int TX = 32;
+    static constexpr int TYc = TY, TZc = TZ;
     static constexpr int THREADS = NT, WARPS = NT / 32;
     static_assert(TY * TZ % WARPS == 0, "rows must divide among the warps");
     static constexpr int ROWS_PER_THREAD = TY * TZ / WARPS;
+    static constexpr int pitch(int w) { return ODD && w % 2 == 0 ? w + 1 : w; }
     // velocity boxes: u on x-faces [x0-1, x0+TX+1] x cells [y0-3, y0+TY+2] x [z0-3, z0+TZ+2];
     // v on cells [x0-3, x0+TX+2] x y-faces [y0-1, y0+TY+1] x cells [z0-3, z0+TZ+2];
     // w on cells [x0-3, x0+TX+2] x [y0-3, y0+TY+2] x z-faces [z0-1, z0+TZ+1]
-    static constexpr int UW = TX + 3, UH = TY + 6, UD = TZ + 6;
-    static constexpr int VW = TX + 6, VH = TY + 3, VD = TZ + 6;
-    static constexpr int WW = TX + 6, WH = TY + 6, WD = TZ + 3;
+    // (UC, VC, WC, MC columns are staged per row; UW, VW, WW, MW are the row pitches)
+    static constexpr int UC = TX + 3, VC = TX + 6, WC = TX + 6, MC = TX + 2;
+    static constexpr int UW = pitch(UC), UH = TY + 6, UD = TZ + 6;
+    static constexpr int VW = pitch(VC), VH = TY + 3, VD = TZ + 6;
+    static constexpr int WW = pitch(WC), WH = TY + 6, WD = TZ + 3;
     // impulse boxes: each component on its faces / cells [lo-1, hi] along every axis
-    static constexpr int MW = TX + 2, MH = TY + 2, MD = TZ + 2;
+    static constexpr int MW = pitch(MC), MH = TY + 2, MD = TZ + 2;
     static constexpr int NU = UW * UH * UD, NV = VW * VH * VD, NW = WW * WH * WD, NM = MW * MH * MD;
     static constexpr int NK = (TX + 1) * (TY + 1) * (TZ + 1);  // cells [x0-1, x0+TX) x [y0-1, y0+TY) x [z0-1, z0+TZ)
     // table slices: indices [lo-2, lo+T+2] of each axis
@@ -72,24 +80,25 @@ __device__ __forceinline__ int box_row_base(int row, int ys, int zs, int ex, int
 }
 
 // Stage a W x H x D box of a face array whose x-extent is ex and corner x is xs, coordinates clamped into the
-// array, from the row offsets `rowbase` (box_row_base).  Each thread keeps one column (its x offset and clamp)
-// and steps through the rows NT / W at a time.
-template <class T, int W, int H, int D, int NT>
+// array, from the row offsets `rowbase` (box_row_base), rows P apart in `dst`.  Each thread keeps one column (its
+// x offset and clamp) and steps through the rows NT / W at a time.
+template <class T, int W, int P, int H, int D, int NT>
 __device__ __forceinline__ void stage_box(T* dst, const int* rowbase, const T* __restrict__ m, int xs, int ex) {
     constexpr int RPS = NT / W, ROWS = H * D;
     const int t = threadIdx.x;
     if (t >= RPS * W) return;
     const int ix = t % W;
     const int gx = clampi(xs + ix, 0, ex - 1);
-    for (int row = t / W; row < ROWS; row += RPS) cp_async_elem<sizeof(T)>(dst + row * W + ix, m + rowbase[row] + gx);
+    for (int row = t / W; row < ROWS; row += RPS) cp_async_elem<sizeof(T)>(dst + row * P + ix, m + rowbase[row] + gx);
 }
-// Stage 0's gauge-reset blend of a staged impulse box: m <- r m + (1-r) u, with u at the same face from the
-// velocity box (plane / row strides VP, VW; `uoff` its offset of the impulse box's corner)
-template <class T, int MW, int MH, int MD, int NT, int VW, int VP>
+// Stage 0's gauge-reset blend of a staged impulse box (MC columns, row pitch MW): m <- r m + (1-r) u, with u at
+// the same face from the velocity box (plane / row strides VP, VW; `uoff` its offset of the impulse box's corner)
+template <class T, int MC, int MW, int MH, int MD, int NT, int VW, int VP>
 __device__ __forceinline__ void blend_box(T* mb, const T* vb, int uoff, T r, T omr) {
-    for (int e = threadIdx.x; e < MW * MH * MD; e += NT) {
-        const int ix = e % MW, iy = (e / MW) % MH, iz = e / (MW * MH);
-        mb[e] = r * mb[e] + omr * vb[uoff + iz * VP + iy * VW + ix];
+    for (int e = threadIdx.x; e < MC * MH * MD; e += NT) {
+        const int ix = e % MC, iy = (e / MC) % MH, iz = e / (MC * MH);
+        const int i = (iz * MH + iy) * MW + ix;
+        mb[i] = r * mb[i] + omr * vb[uoff + iz * VP + iy * VW + ix];
     }
 }
 
@@ -160,9 +169,9 @@ template <class T, class G> __device__ __forceinline__ TileArrays<T> tile_arrays
 
 // Everything a tile's faces need before their arithmetic: the staged boxes and table slices, stage 0's blend, K
 // per cell, and the stage constants.  False (in every thread) when the step has failed.
-template <class T, int TY, int TZ, int NT>
+template <class T, class G>
 __device__ bool tile_prologue(const MomentumArgs<T>& a, const Blk& blk, const TileArrays<T>& t, StageConst& sc, T& dt) {
-    using G = TileGeom<TY, TZ, NT>;
+    constexpr int TY = G::TYc, TZ = G::TZc, NT = G::THREADS;
     pdl_launch_dependents();
     pdl_wait();
     constexpr int TX = G::TX;
@@ -191,12 +200,12 @@ __device__ bool tile_prologue(const MomentumArgs<T>& a, const Blk& blk, const Ti
     }
     __syncthreads();
     const int* rbm = rowbase + RU + RV + RW;
-    stage_box<T, UW, UH, G::UD, NT>(SU, rowbase, a.u[X], x0 - 1, nx + 1);
-    stage_box<T, VW, VH, G::VD, NT>(SV, rowbase + RU, a.u[Y], x0 - 3, nx);
-    stage_box<T, WW, WH, G::WD, NT>(SW, rowbase + RU + RV, a.u[Z], x0 - 3, nx);
-    stage_box<T, MW, MH, G::MD, NT>(MX, rbm, a.m[X], x0 - 1, nx + 1);
-    stage_box<T, MW, MH, G::MD, NT>(MY, rbm + RM, a.m[Y], x0 - 1, nx);
-    stage_box<T, MW, MH, G::MD, NT>(MZ, rbm + 2 * RM, a.m[Z], x0 - 1, nx);
+    stage_box<T, G::UC, UW, UH, G::UD, NT>(SU, rowbase, a.u[X], x0 - 1, nx + 1);
+    stage_box<T, G::VC, VW, VH, G::VD, NT>(SV, rowbase + RU, a.u[Y], x0 - 3, nx);
+    stage_box<T, G::WC, WW, WH, G::WD, NT>(SW, rowbase + RU + RV, a.u[Z], x0 - 3, nx);
+    stage_box<T, G::MC, MW, MH, G::MD, NT>(MX, rbm, a.m[X], x0 - 1, nx + 1);
+    stage_box<T, G::MC, MW, MH, G::MD, NT>(MY, rbm + RM, a.m[Y], x0 - 1, nx);
+    stage_box<T, G::MC, MW, MH, G::MD, NT>(MZ, rbm + 2 * RM, a.m[Z], x0 - 1, nx);
     for (int e = threadIdx.x; e < kNumTabs * (G::SX + G::SY + G::SZ); e += NT) {
         int k, i, axis, len, lo;
         if (e < kNumTabs * G::SX) { axis = X; k = e / G::SX; i = e % G::SX; len = G::SX; lo = x0; }
@@ -221,9 +230,9 @@ __device__ bool tile_prologue(const MomentumArgs<T>& a, const Blk& blk, const Ti
     __syncthreads();
     if (failed) return false;
     if (blend) {      // u of each impulse-box cell: the velocity box entry 2 cells further along its cross axes
-        blend_box<T, MW, MH, G::MD, NT, UW, UP>(MX, SU, (2 * UH + 2) * UW, a.r, a.one_minus_r);
-        blend_box<T, MW, MH, G::MD, NT, VW, VP>(MY, SV, 2 * VP + 2, a.r, a.one_minus_r);
-        blend_box<T, MW, MH, G::MD, NT, WW, WP>(MZ, SW, 2 * WW + 2, a.r, a.one_minus_r);
+        blend_box<T, G::MC, MW, MH, G::MD, NT, UW, UP>(MX, SU, (2 * UH + 2) * UW, a.r, a.one_minus_r);
+        blend_box<T, G::MC, MW, MH, G::MD, NT, VW, VP>(MY, SV, 2 * VP + 2, a.r, a.one_minus_r);
+        blend_box<T, G::MC, MW, MH, G::MD, NT, WW, WP>(MZ, SW, 2 * WW + 2, a.r, a.one_minus_r);
         __syncthreads();
     }
 
@@ -252,7 +261,7 @@ __device__ void sweep_tile_body(const MomentumArgs<T>& a, const Blk& blk) {
     const TileArrays<T> ta = tile_arrays<T, G>(smem_raw);
     StageConst sc;
     T dt;
-    if (!tile_prologue<T, TY, TZ, NT>(a, blk, ta, sc, dt)) return;
+    if (!tile_prologue<T, G>(a, blk, ta, sc, dt)) return;
     T *SU = ta.SU, *SV = ta.SV, *SW = ta.SW, *MX = ta.MX, *MY = ta.MY, *MZ = ta.MZ, *Kc = ta.Kc;
     const Params& p = a.p;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
