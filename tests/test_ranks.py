@@ -36,3 +36,15 @@ def test_two_gloo_ranks():
         assert p.exitcode == 0
     assert [r[1] for r in results] == [11.0, 11.0]
     assert results[0][2] == pytest.approx(2 * 1000 * 5 / 0.011)
+
+
+def test_roofline_names_the_running_sweep(monkeypatch):
+    """The bench line's roofline names the sweep kernel the library runs for the workload's precision form: the
+    one-cell tile in FP64, the packed two-cell kernel in the mixed form, or what CAVITY_SWEEP selects."""
+    import bench
+    monkeypatch.delenv('CAVITY_SWEEP', raising=False)
+    assert bench.sweep_kernel_name('fp64') == 'sweep_tile_kernel'
+    assert bench.sweep_kernel_name('mixed') == 'sweep_pair_kernel'
+    for kind, name in (('tile', 'sweep_tile_kernel'), ('face', 'momentum_kernel'), ('march', 'sweep_march_kernel')):
+        monkeypatch.setenv('CAVITY_SWEEP', kind)
+        assert bench.sweep_kernel_name('mixed') == name
