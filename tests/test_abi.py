@@ -73,3 +73,20 @@ def test_field_output_buffer_is_checked():
                 np.zeros((4, 5, 3), dtype=np.float32).transpose(0, 2, 1)):
         with pytest.raises(ValueError):
             _field_buffer((4, 3, 5), 'u', bad)
+
+
+def test_config_from_settings():
+    """make_config copies the settings by field name and packs up to 8 probes (python_api.py's Config record)."""
+    from les_impulse3d_64_b200 import workloads
+    from les_impulse3d_64_b200.api import make_config
+    s = workloads.C2['settings']
+    c = make_config(s)
+    for name in ('nx', 'ny', 'nz', 'lid_shaped', 'impulse_order', 'adaptive_dt', 'grid_stretch'):
+        assert getattr(c, name) == s[name], name
+    for name in ('nu', 'grid_dx_wall', 'cfl_target', 'dt_max', 'reinit_r'):
+        assert getattr(c, name) == s[name], name
+    assert c.n_probes == 8
+    assert [(c.probe_x[k], c.probe_y[k]) for k in range(8)] == list(workloads.PROBES8)
+    many = make_config(dict(s, probes=list(workloads.PROBES8) + [(0.3, 0.3)]))
+    assert many.n_probes == 8
+    assert make_config(dict(s, probes=())).n_probes == 0
